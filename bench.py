@@ -1,0 +1,416 @@
+#!/usr/bin/env python
+"""BLEST B200 benchmark: BFS GTEPS on one B200 (default workload: RMAT scale
+24, edge factor 16, Jaccard window 65536, 64 seeded sources).
+
+One "step" = one BFS from each of the workload's sources (64 for RMAT-24).
+  value : sum of reached undirected edges / device time of the K timed steps
+          (graph resident in HBM, levels written to HBM; CUDA events on the
+          launching stream; BVSS is larger than L2, so no flush is needed)
+  e2e   : the same metric through the public C-ABI call with HOST buffers:
+          each BFS's levels are copied to pinned host memory inside the
+          timed region (blest_bfs with BLEST_MEM_HOST)
+  --impl reference : the reference's own BVSS kernels (compiled from its
+          sources for sm_100a into oracle/_ref) on the identical BVSS,
+          timed by its own convention (launch -> cudaDeviceSynchronize)
+
+Multi-GPU (torchrun): replicas -- every rank runs the same workload on its
+own GPU (weak scaling); time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    # name: (kind, generator, ordering, window, n_sources, description)
+    "rmat24": ("bfs", ("rmat", 24, 16), "jaccard", 65536, 64,
+               "RMAT scale 24 ef 16 (a,b,c)=(.57,.19,.19) seed 1, symmetrised+dedup, seeded id permutation, "
+               "Jaccard window 65536, 64 seeded sources"),
+    "rmat16": ("bfs", ("rmat", 16, 16), "jaccard", 65536, 64,
+               "RMAT scale 16 ef 16, Jaccard window 65536, 64 seeded sources"),
+    "rmat20": ("bfs", ("rmat", 20, 16), "jaccard", 65536, 64, "RMAT scale 20 ef 16, Jaccard window 65536"),
+    "grid4096": ("bfs", ("grid", 4096, 4096), "rcm", 0, 32,
+                 "2D 4096x4096 grid, 5% edges deleted, 0.1% shortcuts, RCM, 32 seeded sources"),
+    "er25": ("bfs", ("er", 25, 32), "rcm", 0, 32, "Erdos-Renyi 2^25 vertices avg degree 32, RCM, 32 sources"),
+    "cc_rmat24": ("cc", ("rmat", 24, 16), "jaccard", 65536, 0, "connected components, RMAT scale 24"),
+}
+
+SEED = 1
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ----------------------------------------------------------------- graph prep
+def prepare(workload: str, cache_dir: Path, rank: int, world: int):
+    """Build (or load from the per-run cache) the reordered CSC, BVSS and
+    pull CSR. Rank 0 builds; other ranks wait for the cache files."""
+    from blest_b200 import Bvss, Csc
+    kind, gen, order, window, nsrc, _ = WORKLOADS[workload]
+    cache_dir.mkdir(parents=True, exist_ok=True)
+    tag = cache_dir / workload
+    done = Path(str(tag) + ".ready")
+    if rank == 0 and not done.exists():
+        t0 = time.time()
+        if gen[0] == "rmat":
+            csc = Csc.rmat(gen[1], gen[2], 0.57, 0.19, 0.19, seed=SEED, permute_seed=SEED)
+        elif gen[0] == "grid":
+            csc = Csc.grid(gen[1], gen[2], 0.05, 0.001, seed=SEED)
+        else:
+            n = 1 << gen[1]
+            csc = Csc.er(n, n * gen[2] // 2, seed=SEED)
+        t1 = time.time()
+        sources = csc.sample_sources(nsrc, SEED) if nsrc else np.zeros(0, np.uint32)
+        inv = csc.reorder(order, window=window or 65536)
+        t2 = time.time()
+        bvss = Bvss.build(csc)
+        t3 = time.time()
+        log(f"[prep] {workload}: generate {t1 - t0:.1f}s reorder {t2 - t1:.1f}s bvss {t3 - t2:.1f}s "
+            f"n={csc.n} nnz={csc.nnz} social={csc.is_social}")
+        csc.save_bin(str(tag) + "_csc.bin")
+        bvss.save_bin(str(tag) + "_bvss.bin")
+        np.save(str(tag) + "_sources.npy", inv[sources] if nsrc else sources)
+        done.write_text("ok")
+    else:
+        deadline = time.time() + 3600
+        while not done.exists():
+            if time.time() > deadline:
+                raise TimeoutError("graph cache not ready")
+            time.sleep(1.0)
+        csc = Csc.load_bin(str(tag) + "_csc.bin")
+        bvss = Bvss.load_bin(str(tag) + "_bvss.bin")
+    sources = np.load(str(tag) + "_sources.npy")
+    csr = csc if csc.is_symmetric() else csc.transpose()
+    return csc, bvss, csr, sources
+
+
+def reached_edges(csr_degrees: np.ndarray, levels: np.ndarray) -> int:
+    """m_R = 1/2 * sum of degrees of reached vertices (each undirected edge once)."""
+    return int(csr_degrees[levels != 0xFFFFFFFF].sum()) // 2
+
+
+def algorithmic_bytes(bvss_arrays: dict, levels: np.ndarray) -> int:
+    """5*S_R + 12*V_R + 4*N_R: slices/vsets of rsets holding a reached vertex,
+    plus one 4-byte level per reached vertex."""
+    reached = np.nonzero(levels != 0xFFFFFFFF)[0]
+    rsets = np.unique(reached >> 3)
+    rp = bvss_arrays["real_ptrs"]
+    ssp = bvss_arrays["slice_set_ptrs"]
+    v_r = int((rp[rsets + 1].astype(np.int64) - rp[rsets]).sum())
+    s_r = int((ssp[rp[rsets + 1]].astype(np.int64) - ssp[rp[rsets]].astype(np.int64)).sum())
+    return 5 * s_r + 12 * v_r + 4 * reached.size
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(workload: str):
+    """DRAM bytes per launch of the BFS kernel from the committed ncu summary
+    (profiles/bfs_<workload>_traffic.md, line 'traffic_bytes_per_launch: X')."""
+    p = ROOT / "profiles" / f"bfs_{workload}_traffic.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            return float(line.split(":", 1)[1])
+    return None
+
+
+# ----------------------------------------------------------------- arms
+def run_b200(args, rank, world):
+    import torch
+    import torch.distributed as dist
+    import blest_b200
+    from blest_b200 import Graph, Workspace
+    from blest_b200._lib import MEM_HOST
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    blest_b200.init(dev)
+    kind, gen, order, window, nsrc, desc = WORKLOADS[args.workload]
+    csc, bvss, csr, sources = prepare(args.workload, Path(args.cache), rank, world)
+    g = Graph(bvss, csr)
+    info = g.info()
+    n = csc.n
+    deg = np.diff(csr.col_ptrs.astype(np.int64))
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+    ws = Workspace(g)
+    out = torch.empty(n, dtype=torch.int32, device="cuda")
+    barrier = (lambda: dist.barrier()) if world > 1 else (lambda: None)
+
+    # Reference answers for m_R (levels are deterministic), outside timing.
+    host_lv = np.empty(n, dtype=np.uint32)
+    mr, algo = [], []
+    arrays = bvss.arrays()
+    for s in sources:
+        ws.bfs(int(s), host_lv, sptr)
+        mr.append(reached_edges(deg, host_lv))
+        algo.append(algorithmic_bytes(arrays, host_lv))
+    # correctness guard on two sources against the CPU oracle (outside timing)
+    if rank == 0 and not args.skip_check:
+        import oracle as O
+        for s in sources[:2]:
+            ws.bfs(int(s), host_lv, sptr)
+            want = O.bfs_csc(n, csc.col_ptrs, csc.rows, int(s))
+            if not np.array_equal(host_lv, want):
+                raise SystemExit(f"BFS levels differ from the oracle for source {s}")
+    edges_per_step = sum(mr)
+
+    def step(events=None):
+        for i, s in enumerate(sources):
+            if events is not None:
+                events[i][0].record(stream)
+            ws.bfs_async(int(s), out.data_ptr(), sptr)
+            if events is not None:
+                events[i][1].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    stream.synchronize()
+    per_bfs = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                for _ in sources] for _ in range(args.steps)]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clocks:
+        t0.record(stream)
+        for k in range(args.steps):
+            step(per_bfs[k])
+        t1.record(stream)
+        stream.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    bfs_ms = [e[0].elapsed_time(e[1]) for evs in per_bfs for e in evs]
+    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms = float(ms_t.item())
+    value = edges_per_step * args.steps * world / (ms * 1e-3) / 1e9
+
+    # e2e: public API, host (pinned) output, copy inside the timed region
+    pinned = torch.empty(n, dtype=torch.int32, pin_memory=True)
+    pin_np = pinned.numpy().view(np.uint32)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for s in sources[: min(4, len(sources))]:
+        ws.bfs(int(s), pin_np, sptr)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        for s in sources:
+            ws.bfs(int(s), pin_np, sptr)
+    e1.record(stream)
+    stream.synchronize()
+    e2e_ms_t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(e2e_ms_t, op=dist.ReduceOp.MAX)
+    e2e_ms = float(e2e_ms_t.item())
+    e2e = edges_per_step * args.steps * world / (e2e_ms * 1e-3) / 1e9
+
+    peak, peak_kind = measured_peak()
+    avg_bytes = float(np.mean(algo))
+    avg_launch_s = float(np.mean(bfs_ms)) * 1e-3
+    achieved = avg_bytes / avg_launch_s / 1e9
+    traffic = profiled_traffic(args.workload)
+    result = {
+        "metric": "BFS GTEPS (single-source, direction-optimising BVSS BFS)",
+        "value": round(value, 3), "unit": "GTEPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generator; see config)",
+        "config": {"workload": args.workload, "description": desc, "n": n, "nnz_directed": csc.nnz,
+                   "undirected_edges": csc.nnz // 2, "sources_per_step": int(len(sources)),
+                   "reached_edges_per_step": edges_per_step, "bvss_slices": int(info.no_slices),
+                   "graph_bytes_hbm": int(info.device_bytes_graph),
+                   "l2": "inputs larger than L2 (BVSS+CSR in HBM), no flush",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "e2e": {"value": round(e2e, 3), "unit": "GTEPS", "h2d_bytes_per_step": 4 * int(len(sources)),
+                "d2h_bytes_per_step": 4 * n * int(len(sources))},
+        "gpu_launches": 3 * int(len(sources)) * args.steps,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                     "traffic": traffic, "algorithmic_bytes_per_launch": int(avg_bytes),
+                     "avg_launch_ms": round(avg_launch_s * 1e3, 4)},
+    }
+    clk = clocks.summary()
+    result["clocks"] = clk
+    if rank == 0 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(csc, csr, sources, deg, args)
+    return result
+
+
+def cpu_baseline(csc, csr, sources, deg, args):
+    """OpenMP direction-optimising BFS (the oracle's CPU baseline) on the
+    host cores, over a bounded sample of the sources (~10-30 s)."""
+    import oracle as O
+    n = csc.n
+    t_ptrs, t_ids = csr.col_ptrs, csr.rows
+    edges, secs, used, done = 0, 0.0, 0, 0
+    budget = args.cpu_budget
+    for s in sources:
+        t = time.perf_counter()
+        lv, used = O.bfs_omp(n, csc.col_ptrs, csc.rows, t_ptrs, t_ids, int(s), 0)
+        secs += time.perf_counter() - t
+        edges += reached_edges(deg, lv)
+        done += 1
+        if secs > budget:
+            break
+    return {"value": round(edges / secs / 1e9, 4), "unit": "GTEPS", "cores": used, "kind": "port",
+            "sample": f"{done} of {len(sources)} sources, {secs:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    """The reference's BVSSBFSKernel::hostCode (kernels compiled from the
+    reference's sources for sm_100a) on the identical BVSS; rank 0 only."""
+    if rank != 0:
+        return None
+    import oracle as O
+    if not O.ref_available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libblest_ref.so was not built (no reference sources)"}
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    kind, gen, order, window, nsrc, desc = WORKLOADS[args.workload]
+    csc, bvss, csr, sources = prepare(args.workload, Path(args.cache), 0, 1)
+    n = csc.n
+    deg = np.diff(csr.col_ptrs.astype(np.int64))
+    ref = O.RefGraph.from_bvss(n, bvss.arrays(), bvss.full_padding, bvss.update_divergence, csr.col_ptrs, csr.rows)
+    sample = sources[: args.ref_sources]
+    variant = ["BVSSBFS8EnhancedSliceSize8NoMasks4", "FullPad", "LazySwitching", "LazyFullPad"][ref.bfs_variant()]
+    mr = {}
+    for _ in range(args.warmup):
+        for s in sample[:2]:
+            ref.bfs(int(s), n)
+    tot_t, tot_e = 0.0, 0
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+        for _ in range(args.steps):
+            for s in sample:
+                lv, t, _, _ = ref.bfs(int(s), n)
+                if int(s) not in mr:
+                    mr[int(s)] = reached_edges(deg, lv)
+                tot_t += t
+                tot_e += mr[int(s)]
+    value = tot_e / tot_t / 1e9
+    return {
+        "impl": "reference", "metric": "BFS GTEPS (single-source, direction-optimising BVSS BFS)",
+        "value": round(value, 3), "unit": "GTEPS", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(tot_t * 1e3 / args.steps, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generator; see config)",
+        "config": {"workload": args.workload, "description": desc, "n": n, "sources_per_step": int(len(sample)),
+                   "reference_kernel": variant,
+                   "timing": "reference convention: omp_get_wtime launch -> cudaDeviceSynchronize "
+                             "(BFS/BVSSBFSKernel.cuh:1469,1545-1548); graph upload per call untimed"},
+        "cpu_baseline": {"value": round(value, 3), "unit": "GTEPS", "cores": 0, "kind": "reference",
+                         "sample": f"{len(sample)} sources x {args.steps} steps on the GPU (the reference has "
+                                   f"no CPU BFS; its BVSS kernels built for sm_100a)"},
+        "e2e": {"value": round(value, 3), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "clocks": clocks.summary(),
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="rmat24")
+    ap.add_argument("--cache", default="/tmp/blest_bench_cache")
+    ap.add_argument("--ref-sources", type=int, default=16)
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--skip-check", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        log("warmup raised to 3 (minimum)")
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        if args.impl == "reference":
+            res = run_reference(args, rank, world)
+        else:
+            res = run_b200(args, rank, world)
+        if rank == 0 and res is not None:
+            print(json.dumps(res), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,16 @@
+"""B200-native BLEST: BVSS BFS / CC / multi-source BFS on sm_100a.
+
+Layers:
+  - C++ host layer (CSC, RCM / windowed-Jaccard orderings, BVSS builder) and
+    hand-written sm_100a kernels, in libblest_b200.so behind the C ABI of
+    include/blest.h;
+  - blest_b200.graph: Python objects over that ABI;
+  - blest_b200.kernels: the reference's plugin interface (BFSKernel /
+    CCKernel / MBFSKernel with hostCode / run) over the B200 kernels;
+  - blest_b200.server: continuous-batching query server.
+"""
+from ._lib import BlestError, lib  # noqa: F401  (raises ImportError if the .so is missing)
+from .graph import Bvss, Csc, Graph, Workspace, bfs_params, init, load_ordering, relabel_dense, save_ordering  # noqa: F401,E501
+
+__all__ = ["BlestError", "Bvss", "Csc", "Graph", "Workspace", "bfs_params", "init", "load_ordering", "relabel_dense",
+           "save_ordering", "lib"]

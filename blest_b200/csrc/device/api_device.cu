@@ -1,0 +1,414 @@
+// C ABI of the device layer: device selection, resident graphs,
+// workspaces, and the BFS/CC entry points (see include/blest.h).
+#include <cuda_runtime.h>
+#include <omp.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../host/errors.hpp"
+#include "blest.h"
+#include "common.cuh"
+#include "runtime.hpp"
+
+namespace blest {
+
+void check_cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return;
+    const int code = (e == cudaErrorMemoryAllocation) ? BLEST_ERR_OOM
+                     : (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) ? BLEST_ERR_NO_DEVICE
+                                                                                     : BLEST_ERR_CUDA;
+    throw Error(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int device_sm_count(int device) {
+    int sms = 0;
+    BLEST_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    return sms;
+}
+
+namespace {
+
+template <class T>
+T* dev_alloc(blest_graph* g, size_t count) {
+    void* p = nullptr;
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    BLEST_CUDA(cudaMalloc(&p, bytes));
+    g->allocations.push_back(p);
+    g->graph_bytes += bytes;
+    return (T*)p;
+}
+
+template <class T>
+T* upload(blest_graph* g, const T* src, size_t count) {
+    T* d = dev_alloc<T>(g, count);
+    if (count) BLEST_CUDA(cudaMemcpy(d, src, count * sizeof(T), cudaMemcpyHostToDevice));
+    return d;
+}
+
+// Structural checks the kernels rely on for memory safety (every index
+// they dereference is in range), done once at upload.
+void validate_views(const blest_bvss_view* v, const blest_csr_view* c) {
+    auto bad = [](const std::string& m) { throw Error(BLEST_ERR_INVALID_ARG, "invalid graph: " + m); };
+    if (v->slice_size != kSliceSize || v->no_masks != kNoMasks) bad("only slice size 8 with 4 masks is supported");
+    if (v->n == 0) bad("empty graph");
+    if (v->n >= (1u << 28)) throw Error(BLEST_ERR_UNSUPPORTED, "graphs with 2^28 or more vertices are not supported");
+    if (v->no_real_slice_sets != (v->n + 7) / 8) bad("no_real_slice_sets != ceil(n/8)");
+    if (v->no_slices % 4) bad("slice count not a multiple of 4");
+    if (v->no_slices / 4 >= 0xFFFFFFFFull) throw Error(BLEST_ERR_UNSUPPORTED, "more than 2^32-1 tiles");
+    if (!v->slice_set_ptrs || !v->real_ptrs || (v->no_virtual_slice_sets && !v->virtual_to_real) ||
+        (v->no_slices && (!v->row_ids || !v->masks)))
+        bad("null BVSS array");
+    const uint32_t V = v->no_virtual_slice_sets, R = v->no_real_slice_sets;
+    if (v->slice_set_ptrs[0] != 0 || v->slice_set_ptrs[V] != v->no_slices) bad("slice_set_ptrs ends");
+    if (v->real_ptrs[0] != 0 || v->real_ptrs[R] != V) bad("real_ptrs ends");
+    int err = 0;
+#pragma omp parallel for reduction(| : err) schedule(static, 4096)
+    for (int64_t i = 0; i < (int64_t)V; ++i) {
+        const uint64_t a = v->slice_set_ptrs[i], b = v->slice_set_ptrs[i + 1];
+        if (a > b || (a & 3) || v->virtual_to_real[i] >= R) err |= 1;
+    }
+#pragma omp parallel for reduction(| : err) schedule(static, 4096)
+    for (int64_t r = 0; r < (int64_t)R; ++r) {
+        if (v->real_ptrs[r] > v->real_ptrs[r + 1]) err |= 2;
+        else
+            for (uint32_t x = v->real_ptrs[r]; x < v->real_ptrs[r + 1]; ++x)
+                if (v->virtual_to_real[x] != (uint32_t)r) err |= 2;
+    }
+    const uint32_t tailValid = (v->n % 8) ? ((1u << (v->n % 8)) - 1) : 0xFFu;
+#pragma omp parallel for reduction(| : err) schedule(static, 1 << 16)
+    for (int64_t s = 0; s < (int64_t)v->no_slices; ++s) {
+        const uint32_t row = v->row_ids[s];
+        const uint32_t mb = (v->masks[s >> 2] >> (8 * (s & 3))) & 0xFFu;
+        if (mb && row >= v->n) err |= 4;
+    }
+    // mask bits for columns >= n (last rset)
+    {
+        const uint32_t r = R - 1;
+        for (uint32_t x = v->real_ptrs[r]; x < v->real_ptrs[r + 1]; ++x)
+            for (uint64_t s = v->slice_set_ptrs[x]; s < v->slice_set_ptrs[x + 1]; ++s)
+                if (((v->masks[s >> 2] >> (8 * (s & 3))) & 0xFFu) & ~tailValid) err |= 8;
+    }
+    if (err & 1) bad("slice_set_ptrs not non-decreasing multiples of 4, or virtual_to_real out of range");
+    if (err & 2) bad("real_ptrs / virtual_to_real inconsistent");
+    if (err & 4) bad("slice with mask bits and row id out of range");
+    if (err & 8) bad("mask bit for a column >= n");
+    if (!c) bad("the pull CSR is required (pass the transpose; for a symmetric graph, the CSC itself)");
+    if (c->n != v->n) bad("CSR vertex count differs from the BVSS");
+    if (!c->row_ptrs || (c->nnz && !c->col_ids)) bad("null CSR array");
+    if (c->row_ptrs[0] != 0 || c->row_ptrs[c->n] != c->nnz) bad("CSR row_ptrs ends");
+#pragma omp parallel for reduction(| : err) schedule(static, 4096)
+    for (int64_t u = 0; u < (int64_t)c->n; ++u)
+        if (c->row_ptrs[u] > c->row_ptrs[u + 1]) err |= 16;
+#pragma omp parallel for reduction(| : err) schedule(static, 1 << 16)
+    for (int64_t p = 0; p < (int64_t)c->nnz; ++p)
+        if (c->col_ids[p] >= c->n) err |= 32;
+    if (err & 16) bad("CSR row_ptrs not non-decreasing");
+    if (err & 32) bad("CSR column id out of range");
+}
+
+int g_device = -1;
+
+}  // namespace
+
+void workspace_alloc(const blest_graph* g, Workspace& w) {
+    const uint32_t n = g->d.n;
+    w.words = (((n + 31) / 32) + 3) & ~3u;
+    w.qcap = g->d.no_real * 8 + 64;
+    auto alloc = [&](void** p, size_t bytes) {
+        BLEST_CUDA(cudaMalloc(p, std::max<size_t>(bytes, 16)));
+        w.bytes += bytes;
+    };
+    alloc((void**)&w.visited, 4ull * w.words);
+    for (int i = 0; i < 3; ++i) alloc((void**)&w.frontier[i], 4ull * w.words);
+    alloc((void**)&w.q_rset, 4ull * w.qcap);
+    alloc((void**)&w.q_off, 4ull * w.qcap);
+    alloc((void**)&w.counters, sizeof(dev::RunCounters));
+    alloc((void**)&w.levels, 4ull * n);
+    alloc((void**)&w.parents, 4ull * n);
+    alloc((void**)&w.labels_old, 4ull * n);
+    BLEST_CUDA(cudaMallocHost((void**)&w.host_counters, sizeof(dev::RunCounters)));
+    BLEST_CUDA(cudaEventCreate(&w.ev_start));
+    BLEST_CUDA(cudaEventCreate(&w.ev_stop));
+}
+
+void workspace_free(Workspace& w) {
+    cudaFree(w.visited);
+    for (auto& f : w.frontier) cudaFree(f);
+    cudaFree(w.q_rset);
+    cudaFree(w.q_off);
+    cudaFree(w.counters);
+    cudaFree(w.levels);
+    cudaFree(w.parents);
+    cudaFree(w.labels_old);
+    if (w.host_counters) cudaFreeHost(w.host_counters);
+    if (w.ev_start) cudaEventDestroy(w.ev_start);
+    if (w.ev_stop) cudaEventDestroy(w.ev_stop);
+    w = Workspace{};
+}
+
+}  // namespace blest
+
+using blest::guarded;
+
+namespace {
+
+void ensure_device() {
+    if (blest::g_device < 0) {
+        int count = 0;
+        const cudaError_t e = cudaGetDeviceCount(&count);
+        if (e != cudaSuccess || count == 0)
+            throw blest::Error(BLEST_ERR_NO_DEVICE, "no CUDA device available (the CUDA path has no CPU fallback)");
+        BLEST_CUDA(cudaSetDevice(0));
+        blest::g_device = 0;
+    } else {
+        BLEST_CUDA(cudaSetDevice(blest::g_device));
+    }
+}
+
+blest_bfs_params default_bfs_params() {
+    blest_bfs_params p{};
+    p.direction = BLEST_DIR_AUTO;
+    p.slice_test = BLEST_TEST_CUDA_CORE;
+    return p;
+}
+
+void fill_bfs_stats(const blest::Workspace& w, uint32_t src, float ms, blest_bfs_stats* st) {
+    const blest::dev::RunCounters& c = *w.host_counters;
+    if (c.error) throw blest::Error((int)c.error, c.error == BLEST_ERR_BARRIER_TIMEOUT
+                                                      ? "device grid barrier timed out"
+                                                      : (c.error == BLEST_ERR_LEVEL_CAP ? "BFS exceeded n + 1 levels"
+                                                                                         : "device reported an out-of-range index"));
+    if (!st) return;
+    st->time = ms * 1e-3;
+    st->source_vertex = src;
+    st->total_levels = c.levels;
+    st->no_visited = (uint32_t)c.discovered;
+    st->push_levels = c.push_levels;
+    st->pull_levels = c.pull_levels;
+    st->reached_degree_sum = c.degree;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* blest_version(void) { return "blest-b200 1.0 (sm_100a)"; }
+
+int blest_init(int device) {
+    return guarded([&] {
+        int count = 0;
+        const cudaError_t e = cudaGetDeviceCount(&count);
+        if (e != cudaSuccess || count == 0)
+            throw blest::Error(BLEST_ERR_NO_DEVICE, "no CUDA device available (the CUDA path has no CPU fallback)");
+        if (device < 0 || device >= count) throw blest::Error(BLEST_ERR_INVALID_ARG, "device index out of range");
+        BLEST_CUDA(cudaSetDevice(device));
+        cudaDeviceProp prop;
+        BLEST_CUDA(cudaGetDeviceProperties(&prop, device));
+        if (prop.major < 10)
+            throw blest::Error(BLEST_ERR_UNSUPPORTED, "this library is built for sm_100a (B200); device is sm_" +
+                                                          std::to_string(prop.major * 10 + prop.minor));
+        blest::g_device = device;
+    });
+}
+
+int blest_graph_create(const blest_bvss_view* bvss, const blest_csr_view* csr, blest_graph** out) {
+    blest_graph* g = nullptr;
+    const int rc = guarded([&] {
+        blest::require(bvss && out, "null argument");
+        ensure_device();
+        blest::validate_views(bvss, csr);
+        g = new blest_graph;
+        g->device = blest::g_device;
+        g->sm_count = blest::device_sm_count(g->device);
+        const uint32_t R = bvss->no_real_slice_sets, V = bvss->no_virtual_slice_sets;
+        // Tile range of every rset (4 slices per tile).
+        std::vector<uint32_t> rsetTile((size_t)R + 1);
+        for (uint32_t r = 0; r <= R; ++r) rsetTile[r] = (uint32_t)(bvss->slice_set_ptrs[bvss->real_ptrs[r]] / 4);
+        blest::dev::DevGraph& d = g->d;
+        d.n = bvss->n;
+        d.no_real = R;
+        d.no_virtual = V;
+        d.no_slices = bvss->no_slices;
+        d.nnz = csr->nnz;
+        d.degree_total = csr->nnz;
+        d.slice_set_ptrs = blest::upload(g, bvss->slice_set_ptrs, (size_t)V + 1);
+        d.virtual_to_real = blest::upload(g, bvss->virtual_to_real, V);
+        d.real_ptrs = blest::upload(g, bvss->real_ptrs, (size_t)R + 1);
+        d.row4 = (const uint4*)blest::upload(g, bvss->row_ids, bvss->no_slices);
+        d.masks = blest::upload(g, bvss->masks, bvss->no_slices / 4);
+        d.rset_tile = blest::upload(g, rsetTile.data(), rsetTile.size());
+        d.csr_ptrs = blest::upload(g, csr->row_ptrs, (size_t)csr->n + 1);
+        d.csr_ids = blest::upload(g, csr->col_ids, csr->nnz);
+        g->undirected_edges = csr->nnz / 2;
+        BLEST_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+        g->owns_stream = true;
+        g->default_ws = new blest_workspace;
+        g->default_ws->g = g;
+        blest::workspace_alloc(g, g->default_ws->w);
+        *out = g;
+    });
+    if (rc != BLEST_OK && g) blest_graph_destroy(g);
+    return rc;
+}
+
+int blest_graph_destroy(blest_graph* g) {
+    if (!g) return BLEST_OK;
+    cudaSetDevice(g->device);
+    if (g->stream) cudaStreamSynchronize(g->stream);
+    if (g->default_ws) {
+        blest::workspace_free(g->default_ws->w);
+        delete g->default_ws;
+    }
+    for (void* p : g->allocations) cudaFree(p);
+    if (g->stream && g->owns_stream) cudaStreamDestroy(g->stream);
+    delete g;
+    return BLEST_OK;
+}
+
+int blest_graph_info_get(const blest_graph* g, blest_graph_info* out) {
+    return guarded([&] {
+        blest::require(g && out, "null argument");
+        out->n = g->d.n;
+        out->no_real_slice_sets = g->d.no_real;
+        out->no_virtual_slice_sets = g->d.no_virtual;
+        out->no_slices = g->d.no_slices;
+        out->nnz = g->d.nnz;
+        out->undirected_edges = g->undirected_edges;
+        out->device_bytes_graph = g->graph_bytes;
+        out->device_bytes_workspace = g->default_ws ? g->default_ws->w.bytes : 0;
+        out->device = g->device;
+    });
+}
+
+int blest_graph_set_stream(blest_graph* g, void* stream) {
+    return guarded([&] {
+        blest::require(g, "null argument");
+        BLEST_CUDA(cudaStreamSynchronize(g->stream));
+        if (g->owns_stream) BLEST_CUDA(cudaStreamDestroy(g->stream));
+        g->stream = (cudaStream_t)stream;
+        g->owns_stream = false;
+    });
+}
+
+int blest_workspace_create(const blest_graph* g, blest_workspace** out) {
+    blest_workspace* ws = nullptr;
+    const int rc = guarded([&] {
+        blest::require(g && out, "null argument");
+        BLEST_CUDA(cudaSetDevice(g->device));
+        ws = new blest_workspace;
+        ws->g = g;
+        blest::workspace_alloc(g, ws->w);
+        *out = ws;
+    });
+    if (rc != BLEST_OK && ws) blest_workspace_destroy(ws);
+    return rc;
+}
+
+int blest_workspace_destroy(blest_workspace* ws) {
+    if (!ws) return BLEST_OK;
+    cudaSetDevice(ws->g->device);
+    blest::workspace_free(ws->w);
+    delete ws;
+    return BLEST_OK;
+}
+
+int blest_bfs_ws(blest_workspace* ws, uint32_t source, uint32_t* levels_out, uint32_t* parents_out, int out_mem,
+                 const blest_bfs_params* params, void* stream, int async, blest_bfs_stats* stats) {
+    return guarded([&] {
+        blest::require(ws && levels_out, "null argument");
+        blest::require(out_mem == BLEST_MEM_HOST || out_mem == BLEST_MEM_DEVICE, "bad out_mem");
+        const blest_graph* g = ws->g;
+        if (source >= g->d.n) throw blest::Error(BLEST_ERR_INVALID_ARG, "source vertex out of range");
+        BLEST_CUDA(cudaSetDevice(g->device));
+        const blest_bfs_params p = params ? *params : default_bfs_params();
+        blest::require(p.direction >= BLEST_DIR_AUTO && p.direction <= BLEST_DIR_PULL, "bad direction");
+        blest::require(p.slice_test == BLEST_TEST_CUDA_CORE || p.slice_test == BLEST_TEST_B1_MMA, "bad slice_test");
+        cudaStream_t s = stream ? (cudaStream_t)stream : (ws->stream ? ws->stream : g->stream);
+        blest::Workspace& w = ws->w;
+        uint32_t* dl = out_mem == BLEST_MEM_DEVICE ? levels_out : w.levels;
+        uint32_t* dp = parents_out ? (out_mem == BLEST_MEM_DEVICE ? parents_out : w.parents) : nullptr;
+        BLEST_CUDA(cudaEventRecord(w.ev_start, s));
+        blest::launch_bfs(g, w, source, dl, dp, p, s);
+        BLEST_CUDA(cudaEventRecord(w.ev_stop, s));
+        BLEST_CUDA(cudaMemcpyAsync(w.host_counters, w.counters, sizeof(blest::dev::RunCounters),
+                                   cudaMemcpyDeviceToHost, s));
+        if (out_mem == BLEST_MEM_HOST) {
+            BLEST_CUDA(cudaMemcpyAsync(levels_out, dl, 4ull * g->d.n, cudaMemcpyDeviceToHost, s));
+            if (parents_out) BLEST_CUDA(cudaMemcpyAsync(parents_out, dp, 4ull * g->d.n, cudaMemcpyDeviceToHost, s));
+        }
+        ws->pending = true;
+        ws->pending_src = source;
+        ws->stream = s;
+        if (async) return;
+        BLEST_CUDA(cudaStreamSynchronize(s));
+        ws->pending = false;
+        float ms = 0;
+        BLEST_CUDA(cudaEventElapsedTime(&ms, w.ev_start, w.ev_stop));
+        fill_bfs_stats(w, source, ms, stats);
+    });
+}
+
+int blest_workspace_sync(blest_workspace* ws, blest_bfs_stats* stats) {
+    return guarded([&] {
+        blest::require(ws, "null argument");
+        if (!ws->pending) return;
+        BLEST_CUDA(cudaStreamSynchronize(ws->stream));
+        ws->pending = false;
+        float ms = 0;
+        BLEST_CUDA(cudaEventElapsedTime(&ms, ws->w.ev_start, ws->w.ev_stop));
+        fill_bfs_stats(ws->w, ws->pending_src, ms, stats);
+    });
+}
+
+int blest_bfs(blest_graph* g, uint32_t source, uint32_t* levels_out, uint32_t* parents_out, int out_mem,
+              const blest_bfs_params* params, blest_bfs_stats* stats) {
+    if (!g) {
+        blest::set_last_error("null graph");
+        return BLEST_ERR_INVALID_ARG;
+    }
+    return blest_bfs_ws(g->default_ws, source, levels_out, parents_out, out_mem, params, g->stream, 0, stats);
+}
+
+int blest_cc_ws(blest_workspace* ws, uint32_t* labels_out, int out_mem, void* stream, blest_cc_stats* stats) {
+    return guarded([&] {
+        blest::require(ws && labels_out, "null argument");
+        blest::require(out_mem == BLEST_MEM_HOST || out_mem == BLEST_MEM_DEVICE, "bad out_mem");
+        const blest_graph* g = ws->g;
+        BLEST_CUDA(cudaSetDevice(g->device));
+        cudaStream_t s = stream ? (cudaStream_t)stream : (ws->stream ? ws->stream : g->stream);
+        blest::Workspace& w = ws->w;
+        uint32_t* dl = out_mem == BLEST_MEM_DEVICE ? labels_out : w.levels;
+        BLEST_CUDA(cudaEventRecord(w.ev_start, s));
+        blest::launch_cc(g, w, dl, s);
+        BLEST_CUDA(cudaEventRecord(w.ev_stop, s));
+        BLEST_CUDA(cudaMemcpyAsync(w.host_counters, w.counters, sizeof(blest::dev::RunCounters),
+                                   cudaMemcpyDeviceToHost, s));
+        if (out_mem == BLEST_MEM_HOST)
+            BLEST_CUDA(cudaMemcpyAsync(labels_out, dl, 4ull * g->d.n, cudaMemcpyDeviceToHost, s));
+        BLEST_CUDA(cudaStreamSynchronize(s));
+        const blest::dev::RunCounters& c = *w.host_counters;
+        if (c.error)
+            throw blest::Error((int)c.error, c.error == BLEST_ERR_BARRIER_TIMEOUT ? "device grid barrier timed out"
+                                                                                 : "CC did not converge within n + 1 iterations");
+        float ms = 0;
+        BLEST_CUDA(cudaEventElapsedTime(&ms, w.ev_start, w.ev_stop));
+        if (stats) {
+            stats->time = ms * 1e-3;
+            stats->no_components = (uint32_t)c.discovered;
+            stats->iterations = c.iterations;
+        }
+    });
+}
+
+int blest_cc(blest_graph* g, uint32_t* labels_out, int out_mem, blest_cc_stats* stats) {
+    if (!g) {
+        blest::set_last_error("null graph");
+        return BLEST_ERR_INVALID_ARG;
+    }
+    return blest_cc_ws(g->default_ws, labels_out, out_mem, g->stream, stats);
+}
+
+}  // extern "C"

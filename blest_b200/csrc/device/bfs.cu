@@ -1,0 +1,459 @@
+// Single-source direction-optimising BFS over BVSS tiles (push) and CSR
+// in-neighbour lists (pull), as ONE persistent cooperative kernel per BFS.
+//
+// Replaces the six BFS kernels of BFS/BVSSBFSKernel.cuh (:33-1261) and the
+// launcher BVSSBFSKernel::hostCode (:1283-1608). Results are the same
+// levels (0 at the source, 0xFFFFFFFF unreached); the schedule differs:
+//  - Discovery is eager (atomicOr on the visited bitmap decides the
+//    winner, which writes the level), so a level needs no full-bitmap sweep
+//    and only ONE grid barrier (the reference's lazy kernels sweep all n/32
+//    words and sync three times per level, :204-283).
+//  - The frontier is a cumulative queue of real slice sets (rsets) with the
+//    running number of tiles in front of each entry, so a level's push work
+//    is a flat range of tiles split evenly over all warps (the reference
+//    gives each warp one 128-slice vset, :133-203).
+//  - Frontier bitmaps are triple-buffered and cleared sparsely through the
+//    queue of two levels back, never by an O(n) pass.
+//  - The direction switch uses Beamer's edge/vertex units
+//    (m_f * alpha > m_u to pull, n_f * beta < n back to push) instead of
+//    the reference's unvisited-vertices vs frontier-vsets test (:96).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "runtime.hpp"
+#include "../host/common.hpp"
+
+namespace blest {
+namespace dev {
+
+struct BfsArgs {
+    DevGraph g;
+    uint32_t* levels;
+    uint32_t* parents;
+    uint32_t* visited;
+    uint32_t* frontier0;
+    uint32_t* frontier1;
+    uint32_t* frontier2;
+    uint32_t* q_rset;
+    uint32_t* q_off;
+    RunCounters* ctr;
+    uint32_t words;
+    uint32_t src;
+    int direction;
+    float alpha;
+    float beta;
+};
+
+__device__ __forceinline__ uint32_t* frontier_buf(const BfsArgs& a, uint32_t level) {
+    const uint32_t m = level % 3;
+    return m == 0 ? a.frontier0 : (m == 1 ? a.frontier1 : a.frontier2);
+}
+
+// Work units of one queued rset: tiles (packed mode) or 32-tile chunks
+// (rset-aligned mode, needed when one warp must share a frontier byte).
+template <bool ALIGNED>
+__device__ __forceinline__ uint32_t rset_units(const DevGraph& g, uint32_t r) {
+    const uint32_t t = __ldg(&g.rset_tile[r + 1]) - __ldg(&g.rset_tile[r]);
+    return ALIGNED ? (t + 31) / 32 : t;
+}
+
+__global__ void bfs_init_kernel(BfsArgs a) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t nth = gridDim.x * blockDim.x;
+    const uint32_t n = a.g.n, src = a.src;
+    for (uint32_t v = tid; v < n; v += nth) {
+        a.levels[v] = v == src ? 0u : kUnreached;
+        if (a.parents) a.parents[v] = v == src ? src : kUnreached;
+    }
+    const uint32_t sw = src >> 5, sb = 1u << (src & 31);
+    for (uint32_t i = tid; i < a.words; i += nth) {
+        a.visited[i] = i == sw ? sb : 0u;
+        a.frontier0[i] = i == sw ? sb : 0u;
+        a.frontier1[i] = 0u;
+        a.frontier2[i] = 0u;
+    }
+}
+
+// Writes the level-0 state; one thread (after bfs_init_kernel).
+template <bool ALIGNED>
+__global__ void bfs_seed_kernel(BfsArgs a) {
+    RunCounters* c = a.ctr;
+    const uint32_t r = a.src >> 3;
+    const uint32_t units = rset_units<ALIGNED>(a.g, r);
+    uint64_t q = 0;
+    if (units) {
+        a.q_rset[0] = r;
+        a.q_off[0] = 0;
+        q = (1ull << kQShift) | units;
+    }
+    const uint64_t deg = a.g.csr_ptrs[a.src + 1] - a.g.csr_ptrs[a.src];
+    c->queue = q;
+    c->discovered = 1;
+    c->degree = deg;
+    c->grab[0] = c->grab[1] = 0;
+    c->bar_count = 0;
+    c->bar_gen = 0;
+    c->error = 0;
+    c->levels = 0;
+    c->push_levels = 0;
+    c->pull_levels = 0;
+    c->iterations = 0;
+    c->snap_queue[0] = q;
+    c->snap_discovered[0] = 1;
+    c->snap_degree[0] = deg;
+    c->snap_queue[1] = c->snap_discovered[1] = c->snap_degree[1] = 0;
+}
+
+// Per-warp accumulator of enqueue requests, flushed with one atomic.
+struct Enqueue {
+    uint32_t rset[4];
+    uint32_t cnt;
+    uint32_t units;
+};
+
+template <bool ALIGNED>
+__device__ __forceinline__ void flush_enqueue(const BfsArgs& a, Enqueue& q) {
+    const uint32_t lane = threadIdx.x & 31;
+    if (!__any_sync(0xFFFFFFFFu, q.cnt != 0)) return;
+    const uint64_t mine = ((uint64_t)q.cnt << kQShift) | q.units;
+    const uint64_t incl = warp_inclusive_scan64(mine);
+    uint64_t base = 0;
+    if (lane == 31) base = atomicAdd((unsigned long long*)&a.ctr->queue, (unsigned long long)incl);
+    base = __shfl_sync(0xFFFFFFFFu, base, 31);
+    const uint64_t excl = base + incl - mine;
+    uint32_t e = (uint32_t)(excl >> kQShift);
+    uint32_t u = (uint32_t)(excl & kQUnitMask);
+    for (uint32_t i = 0; i < q.cnt; ++i) {
+        const uint32_t r = q.rset[i];
+        a.q_rset[e] = r;
+        a.q_off[e] = u;
+        ++e;
+        u += rset_units<ALIGNED>(a.g, r);
+    }
+    q.cnt = 0;
+    q.units = 0;
+}
+
+// Claim vertex `row` for `level`; the atomicOr on visited decides the
+// single winner, which records level/parent, sets the frontier bit and,
+// when it is the first new vertex of its rset this level, queues the rset.
+template <bool ALIGNED, bool PARENTS>
+__device__ __forceinline__ void discover(const BfsArgs& a, uint32_t* fcur, uint32_t row, uint32_t parent,
+                                         uint32_t level, Enqueue& q, uint32_t& disc, uint64_t& deg) {
+    if (row >= a.g.n) {
+        set_error(a.ctr, BLEST_ERR_DEVICE_INDEX);
+        return;
+    }
+    const uint32_t w = row >> 5, b = 1u << (row & 31);
+    if (__ldcg(&a.visited[w]) & b) return;
+    const uint32_t old = atomicOr(&a.visited[w], b);
+    if (old & b) return;
+    a.levels[row] = level;
+    if (PARENTS) a.parents[row] = parent;
+    ++disc;
+    deg += __ldg(&a.g.csr_ptrs[row + 1]) - __ldg(&a.g.csr_ptrs[row]);
+    const uint32_t oldF = atomicOr(&fcur[w], b);
+    if (((oldF >> (row & 24)) & 0xFFu) == 0) {
+        const uint32_t r = row >> 3;
+        const uint32_t units = rset_units<ALIGNED>(a.g, r);
+        if (units) {
+            q.rset[q.cnt++] = r;
+            q.units += units;
+        }
+    }
+}
+
+// mma.sync m8n8k128 b1 AND+POPC: d[i] = popc(A_row & B_col) per the PTX
+// fragment layout (lane l: A row l/4 bits [32*(l%4), +32), B column l/4
+// bits [32*(l%4), +32), D row l/4 columns 2*(l%4) + {0,1}).
+__device__ __forceinline__ void mma_b1_and_popc(uint32_t a, uint32_t b, uint32_t& d0, uint32_t& d1) {
+    uint32_t c0 = 0, c1 = 0;
+    asm volatile(
+        "mma.sync.aligned.m8n8k128.row.col.s32.b1.b1.s32.and.popc {%0, %1}, {%2}, {%3}, {%4, %5};"
+        : "=r"(d0), "=r"(d1)
+        : "r"(a), "r"(b), "r"(c0), "r"(c1));
+}
+
+// Hit flags of this lane's 4 slices against frontier byte fb, via the b1
+// tensor-core MMA: with A = the lane's mask word, placing fb (shifted to
+// byte k) only in the B column block that lane l's own A chunk meets
+// (B column n uses chunk n/2 only, i.e. lanes l with l%4 == l/8) makes
+// D[l/4][2*(l%4)+i] = popc(byte k_i of lane l's mask & fb). Two MMAs give
+// bytes {0,1} and {2,3}. fb must be warp-uniform.
+__device__ __forceinline__ uint32_t hits_mma(uint32_t mask, uint32_t fb) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t col = lane >> 2, chunk = lane & 3;
+    const bool diag = chunk == (col >> 1);
+    const uint32_t sh = 8u * (col & 1);
+    uint32_t d0, d1, d2, d3;
+    mma_b1_and_popc(mask, diag ? (fb << sh) : 0u, d0, d1);
+    mma_b1_and_popc(mask, diag ? (fb << (16 + sh)) : 0u, d2, d3);
+    return (d0 ? 1u : 0u) | (d1 ? 2u : 0u) | (d2 ? 4u : 0u) | (d3 ? 8u : 0u);
+}
+
+// Largest queue entry e in [lo, hi) with q_off[e] <= pos (q_off sorted).
+__device__ __forceinline__ uint32_t find_owner(const uint32_t* q_off, uint32_t lo, uint32_t hi, uint32_t pos) {
+    const uint32_t lane = threadIdx.x & 31;
+    while (hi - lo > 32) {
+        const uint32_t step = (hi - lo + 31) / 32;
+        const uint32_t idx = lo + lane * step;
+        const bool ok = idx < hi && __ldcg(&q_off[idx]) <= pos;
+        const uint32_t cnt = __popc(__ballot_sync(0xFFFFFFFFu, ok));  // >= 1 (sample 0 == lo)
+        const uint32_t nlo = lo + (cnt - 1) * step;
+        hi = min(hi, nlo + step);
+        lo = nlo;
+    }
+    const uint32_t idx = lo + lane;
+    const bool ok = idx < hi && __ldcg(&q_off[idx]) <= pos;
+    return lo + __popc(__ballot_sync(0xFFFFFFFFu, ok)) - 1;
+}
+
+template <bool ALIGNED, bool MMA, bool PARENTS>
+__global__ void __launch_bounds__(512) bfs_persistent_kernel(BfsArgs a) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t nth = gridDim.x * blockDim.x;
+    const uint32_t warp = tid >> 5;
+    const uint32_t nwarps = nth >> 5;
+    const DevGraph& g = a.g;
+    RunCounters* c = a.ctr;
+
+    // Cumulative counters at the end of levels L-3 and L-2.
+    uint32_t E3 = 0, E2 = 0, U2 = 0;
+    uint64_t D2 = 0, G2 = 0;
+    int dir = a.direction == BLEST_DIR_PULL ? BLEST_DIR_PULL : BLEST_DIR_PUSH;
+
+    for (uint32_t level = 1;; ++level) {
+        const uint32_t par = (level - 1) & 1;
+        const uint64_t q1 = c->snap_queue[par];
+        const uint32_t E1 = (uint32_t)(q1 >> kQShift), U1 = (uint32_t)(q1 & kQUnitMask);
+        const uint64_t D1 = c->snap_discovered[par], G1 = c->snap_degree[par];
+        const uint64_t nf = D1 - D2;  // discovered at level L-1
+        if (nf == 0) {
+            if (tid == 0) c->levels = level - 1;  // max level + 1
+            break;
+        }
+        if (level > g.n + 1) {
+            set_error(c, BLEST_ERR_LEVEL_CAP);
+            break;
+        }
+        if (a.direction == BLEST_DIR_AUTO) {
+            const double mf = (double)(G1 - G2), mu = (double)(g.degree_total - G1);
+            if (dir == BLEST_DIR_PUSH && mf * a.alpha > mu) dir = BLEST_DIR_PULL;
+            else if (dir == BLEST_DIR_PULL && (double)nf * a.beta < (double)g.n) dir = BLEST_DIR_PUSH;
+        }
+        uint32_t* fprev = frontier_buf(a, level - 1);
+        uint32_t* fcur = frontier_buf(a, level);
+        uint8_t* fclr = reinterpret_cast<uint8_t*>(frontier_buf(a, level + 1));
+
+        Enqueue q;
+        q.cnt = 0;
+        q.units = 0;
+        uint32_t disc = 0;
+        uint64_t deg = 0;
+
+        if (dir == BLEST_DIR_PUSH) {
+            const uint32_t total = U1 - U2;
+            const uint32_t per = ALIGNED ? 1u : 32u;  // units per warp step
+            const uint32_t steps = (total + per - 1) / per;
+            const uint32_t k = (steps + nwarps - 1) / nwarps;
+            uint32_t s = warp * k;
+            const uint32_t send = min(steps, s + k);
+            if (s < send) {
+                uint32_t owner = find_owner(a.q_off, E2, E1, U2 + s * per);
+                for (; s < send; ++s) {
+                    const uint32_t base = U2 + s * per;
+                    // Entry bounds for the (up to 32) entries this step can touch.
+                    const uint32_t ei = owner + lane;
+                    const bool in = ei < E1;
+                    const uint32_t eoff = in ? __ldcg(&a.q_off[ei]) : 0xFFFFFFFFu;
+                    const uint32_t ers = in ? __ldcg(&a.q_rset[ei]) : 0u;
+                    uint32_t pos, my;
+                    if (ALIGNED) {
+                        pos = base;
+                        my = 0;
+                        // warp-uniform owner of this chunk
+                        my = __popc(__ballot_sync(0xFFFFFFFFu, eoff <= pos)) - 1;
+                    } else {
+                        pos = base + lane;
+                        uint32_t lo = 0;
+#pragma unroll
+                        for (uint32_t st = 16; st > 0; st >>= 1) {
+                            const uint32_t cand = lo + st;
+                            const uint32_t b = __shfl_sync(0xFFFFFFFFu, eoff, cand & 31);
+                            if (cand < 32 && b <= pos) lo = cand;
+                        }
+                        my = lo;
+                    }
+                    const uint32_t r = __shfl_sync(0xFFFFFFFFu, ers, my);
+                    const uint32_t off = __shfl_sync(0xFFFFFFFFu, eoff, my);
+                    owner += __shfl_sync(0xFFFFFFFFu, my, 31);
+                    const uint32_t t0 = __ldg(&g.rset_tile[r]);
+                    const uint32_t t1 = __ldg(&g.rset_tile[r + 1]);
+                    uint32_t tile;
+                    bool valid;
+                    if (ALIGNED) {
+                        tile = t0 + (pos - off) * 32 + lane;
+                        valid = tile < t1;
+                    } else {
+                        tile = t0 + (pos - off);
+                        valid = pos < U1;
+                    }
+                    if (valid && (pos < off || tile >= t1)) {
+                        // queue offsets inconsistent with the rset's tiles: never read past it
+                        set_error(c, BLEST_ERR_DEVICE_INDEX);
+                        valid = false;
+                    }
+                    const uint32_t fb = (__ldcg(&fprev[r >> 2]) >> (8 * (r & 3))) & 0xFFu;
+                    uint4 rows = make_uint4(0, 0, 0, 0);
+                    uint32_t mask = 0;
+                    if (valid) {
+                        rows = ld_stream(&g.row4[tile]);
+                        mask = ld_stream(&g.masks[tile]);
+                    }
+                    uint32_t hits;
+                    if (MMA) {
+                        hits = hits_mma(mask, fb);
+                    } else {
+                        hits = 0;
+#pragma unroll
+                        for (uint32_t kk = 0; kk < 4; ++kk) hits |= (((mask >> (8 * kk)) & fb & 0xFFu) ? 1u : 0u) << kk;
+                    }
+                    if (hits) {
+                        const uint32_t rowk[4] = {rows.x, rows.y, rows.z, rows.w};
+#pragma unroll
+                        for (uint32_t kk = 0; kk < 4; ++kk) {
+                            if (hits & (1u << kk)) {
+                                const uint32_t hb = (mask >> (8 * kk)) & fb & 0xFFu;
+                                const uint32_t parent = r * 8 + (__ffs(hb) - 1);
+                                discover<ALIGNED, PARENTS>(a, fcur, rowk[kk], parent, level, q, disc, deg);
+                            }
+                        }
+                    }
+                    flush_enqueue<ALIGNED>(a, q);
+                }
+            }
+        } else {
+            // Bottom-up: each warp owns whole 32-vertex words.
+            const uint32_t W = (g.n + 31) / 32;
+            const uint32_t tailMask = (g.n & 31) ? ((1u << (g.n & 31)) - 1) : 0xFFFFFFFFu;
+            for (uint32_t i = warp; i < W; i += nwarps) {
+                const uint32_t vis = __ldcg(&a.visited[i]);
+                const uint32_t unv = ~vis & (i == W - 1 ? tailMask : 0xFFFFFFFFu);
+                if (unv == 0) continue;
+                bool found = false;
+                uint32_t parent = kUnreached;
+                const uint32_t u = i * 32 + lane;
+                if ((unv >> lane) & 1u) {
+                    const uint32_t pb = __ldg(&g.csr_ptrs[u]), pe = __ldg(&g.csr_ptrs[u + 1]);
+                    for (uint32_t p = pb; p < pe; ++p) {
+                        const uint32_t v = __ldg(&g.csr_ids[p]);
+                        if ((__ldcg(&fprev[v >> 5]) >> (v & 31)) & 1u) {
+                            found = true;
+                            parent = v;
+                            break;
+                        }
+                    }
+                }
+                const uint32_t nb = __ballot_sync(0xFFFFFFFFu, found);
+                if (nb == 0) continue;
+                if (lane == 0) {
+                    a.visited[i] = vis | nb;
+                    fcur[i] = nb;
+                }
+                if (found) {
+                    a.levels[u] = level;
+                    if (PARENTS) a.parents[u] = parent;
+                    ++disc;
+                    deg += __ldg(&g.csr_ptrs[u + 1]) - __ldg(&g.csr_ptrs[u]);
+                }
+                if (lane < 4 && ((nb >> (8 * lane)) & 0xFFu)) {
+                    const uint32_t r = i * 4 + lane;
+                    const uint32_t units = rset_units<ALIGNED>(g, r);
+                    if (units) {
+                        q.rset[q.cnt++] = r;
+                        q.units += units;
+                    }
+                }
+                flush_enqueue<ALIGNED>(a, q);
+            }
+        }
+
+        // Clear the frontier bytes written two levels back (queue of L-2).
+        for (uint32_t e = E3 + tid; e < E2; e += nth) fclr[__ldcg(&a.q_rset[e])] = 0;
+
+        const uint64_t wd = warp_sum64(disc), wg = warp_sum64(deg);
+        if (lane == 0 && wd) {
+            atomicAdd((unsigned long long*)&c->discovered, (unsigned long long)wd);
+            atomicAdd((unsigned long long*)&c->degree, (unsigned long long)wg);
+        }
+        if (tid == 0) {
+            if (dir == BLEST_DIR_PUSH) c->push_levels++;
+            else c->pull_levels++;
+        }
+        if (!grid_barrier(c, level & 1)) return;
+        E3 = E2;
+        E2 = E1;
+        U2 = U1;
+        D2 = D1;
+        G2 = G1;
+    }
+}
+
+}  // namespace dev
+
+namespace {
+
+template <bool ALIGNED, bool MMA, bool PARENTS>
+void launch_variant(const blest_graph* g, const dev::BfsArgs& args, int blocks_per_sm, int threads,
+                    cudaStream_t s) {
+    auto kern = dev::bfs_persistent_kernel<ALIGNED, MMA, PARENTS>;
+    int maxBlocks = 0;
+    BLEST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxBlocks, kern, threads, 0));
+    if (maxBlocks < 1) throw Error(BLEST_ERR_CUDA, "BFS kernel cannot be resident with this block size");
+    const int bps = blocks_per_sm > 0 ? std::min(blocks_per_sm, maxBlocks) : maxBlocks;
+    const int grid = bps * g->sm_count;
+    dev::bfs_init_kernel<<<g->sm_count * 4, 512, 0, s>>>(args);
+    BLEST_CUDA(cudaGetLastError());
+    dev::bfs_seed_kernel<ALIGNED><<<1, 1, 0, s>>>(args);
+    BLEST_CUDA(cudaGetLastError());
+    void* kargs[] = {(void*)&args};
+    BLEST_CUDA(cudaLaunchCooperativeKernel((void*)kern, grid, threads, kargs, 0, s));
+}
+
+}  // namespace
+
+void launch_bfs(const blest_graph* g, Workspace& w, uint32_t src, uint32_t* levels, uint32_t* parents,
+                const blest_bfs_params& p, cudaStream_t s) {
+    dev::BfsArgs a{};
+    a.g = g->d;
+    a.levels = levels;
+    a.parents = parents;
+    a.visited = w.visited;
+    a.frontier0 = w.frontier[0];
+    a.frontier1 = w.frontier[1];
+    a.frontier2 = w.frontier[2];
+    a.q_rset = w.q_rset;
+    a.q_off = w.q_off;
+    a.ctr = w.counters;
+    a.words = w.words;
+    a.src = src;
+    a.direction = p.direction;
+    a.alpha = p.alpha > 0 ? (float)p.alpha : 14.0f;
+    a.beta = p.beta > 0 ? (float)p.beta : 24.0f;
+    const int threads = p.threads_per_block > 0 ? p.threads_per_block : 512;
+    if (threads % 32 || threads > 512) throw Error(BLEST_ERR_INVALID_ARG, "threads_per_block must be a multiple of 32, <= 512");
+    const bool mma = p.slice_test == BLEST_TEST_B1_MMA;
+    const bool par = parents != nullptr;
+    if (mma) {
+        if (par) launch_variant<true, true, true>(g, a, p.blocks_per_sm, threads, s);
+        else launch_variant<true, true, false>(g, a, p.blocks_per_sm, threads, s);
+    } else {
+        if (par) launch_variant<false, false, true>(g, a, p.blocks_per_sm, threads, s);
+        else launch_variant<false, false, false>(g, a, p.blocks_per_sm, threads, s);
+    }
+}
+
+}  // namespace blest

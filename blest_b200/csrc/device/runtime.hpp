@@ -1,0 +1,76 @@
+// Host-side runtime objects behind the device C ABI: the resident graph
+// and per-query workspaces.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "blest.h"
+#include "common.cuh"
+#include "../host/common.hpp"
+
+namespace blest {
+
+void check_cuda(cudaError_t e, const char* what);
+#define BLEST_CUDA(x) ::blest::check_cuda((x), #x)
+
+// Scratch of one BFS/CC run. Sized for the graph at creation; every run
+// re-initialises what it uses.
+struct Workspace {
+    uint32_t words = 0;        // ceil(n / 32), rounded up to a multiple of 4
+    uint32_t qcap = 0;         // queue capacity (entries)
+    uint32_t* visited = nullptr;
+    uint32_t* frontier[3] = {nullptr, nullptr, nullptr};
+    uint32_t* q_rset = nullptr;
+    uint32_t* q_off = nullptr;
+    dev::RunCounters* counters = nullptr;
+    uint32_t* levels = nullptr;   // internal output buffers (host-output calls)
+    uint32_t* parents = nullptr;
+    uint32_t* labels_old = nullptr;  // CC
+    dev::RunCounters* host_counters = nullptr;  // pinned mirror
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    uint64_t bytes = 0;
+};
+
+}  // namespace blest
+
+struct blest_graph {
+    int device = 0;
+    int sm_count = 0;
+    blest::dev::DevGraph d{};
+    std::vector<void*> allocations;
+    uint64_t graph_bytes = 0;
+    uint64_t undirected_edges = 0;
+    cudaStream_t stream = nullptr;
+    bool owns_stream = false;
+    blest_workspace* default_ws = nullptr;
+};
+
+struct blest_workspace {
+    const blest_graph* g = nullptr;
+    blest::Workspace w;
+    // async bookkeeping
+    cudaStream_t stream = nullptr;
+    uint32_t pending_src = 0;
+    bool pending = false;
+    uint32_t* pending_levels_host = nullptr;
+    uint32_t* pending_parents_host = nullptr;
+};
+
+namespace blest {
+
+void workspace_alloc(const blest_graph* g, Workspace& w);
+void workspace_free(Workspace& w);
+
+// Kernel launchers (bfs.cu, cc.cu). Outputs are device pointers.
+void launch_bfs(const blest_graph* g, Workspace& w, uint32_t src, uint32_t* levels, uint32_t* parents,
+                const blest_bfs_params& p, cudaStream_t s);
+void launch_cc(const blest_graph* g, Workspace& w, uint32_t* labels, cudaStream_t s);
+
+int device_sm_count(int device);
+
+}  // namespace blest

@@ -1,0 +1,411 @@
+#include "csc.hpp"
+
+#include <omp.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+
+#include "blest.h"
+
+namespace blest {
+
+double Csc::average_degree() const {
+    double average = 0;
+    for (uint32_t j = 0; j < n; ++j) average += degree(j);
+    return n ? average / n : 0.0;
+}
+
+uint32_t Csc::max_degree() const {
+    uint32_t m = 0;
+    for (uint32_t j = 0; j < n; ++j) m = std::max(m, degree(j));
+    return m;
+}
+
+uint32_t Csc::max_bandwidth() const {
+    uint32_t band = 0;
+    for (uint32_t j = 0; j < n; ++j) {
+        if (col_ptrs[j] == col_ptrs[j + 1]) continue;
+        int64_t d = (int64_t)j - (int64_t)rows[col_ptrs[j + 1] - 1];
+        band = std::max<uint32_t>(band, (uint32_t)(d < 0 ? -d : d));
+    }
+    return band;
+}
+
+double Csc::average_bandwidth() const {
+    double average = 0;
+    for (uint32_t j = 0; j < n; ++j) {
+        if (col_ptrs[j] == col_ptrs[j + 1]) continue;
+        int64_t d = (int64_t)j - (int64_t)rows[col_ptrs[j + 1] - 1];
+        average += (uint32_t)(d < 0 ? -d : d);
+    }
+    return n ? average / n : 0.0;
+}
+
+// Restatement of Common.cuh:100-250. The floating-point operations are
+// kept in the reference's order so the decision is the same on the same
+// degree sequence.
+bool is_social_degree_distribution(const std::vector<uint32_t>& deg) {
+    const uint32_t n = (uint32_t)deg.size();
+    if (n == 0) return false;
+    uint32_t maxDeg = 0;
+    unsigned long long sumDeg = 0;
+    for (uint32_t d : deg) {
+        sumDeg += d;
+        maxDeg = std::max(maxDeg, d);
+    }
+    if (maxDeg == 0 || sumDeg == 0) return false;
+
+    std::vector<uint32_t> sorted = deg;
+    std::sort(sorted.begin(), sorted.end());
+    auto shareTop = [&](double frac) {
+        double raw = frac * (double)n;
+        uint32_t k = (uint32_t)std::ceil(raw);
+        if (k == 0) k = 1;
+        if (k > n) k = n;
+        unsigned long long top = 0;
+        for (uint32_t i = 0; i < k; ++i) top += sorted[n - 1 - i];
+        return (double)top / (double)sumDeg;
+    };
+    const bool heavyTail = shareTop(0.01) >= 0.05 && shareTop(0.10) >= 0.40;
+
+    std::vector<uint32_t> freq((size_t)maxDeg + 1, 0);
+    for (uint32_t d : deg) ++freq[d];
+    std::vector<double> xs, ys;
+    for (uint32_t k = 5; k <= maxDeg; ++k) {
+        if (freq[k] != 0) {
+            xs.push_back(std::log((double)k));
+            ys.push_back(std::log((double)freq[k]));
+        }
+    }
+    bool powerLaw = false;
+    const uint32_t m = (uint32_t)xs.size();
+    if (m >= 3u) {
+        double sx = 0, sy = 0, sxy = 0, sxx = 0;
+        for (uint32_t i = 0; i < m; ++i) {
+            sx += xs[i];
+            sy += ys[i];
+            sxy += xs[i] * ys[i];
+            sxx += xs[i] * xs[i];
+        }
+        const double nd = (double)m;
+        const double denom = nd * sxx - sx * sx;
+        if (denom > 0.0) {
+            const double slope = (nd * sxy - sx * sy) / denom;
+            const double intercept = (sy - slope * sx) / nd;
+            const double yMean = sy / nd;
+            double ssTot = 0, ssRes = 0;
+            for (uint32_t i = 0; i < m; ++i) {
+                const double yHat = intercept + slope * xs[i];
+                ssTot += (ys[i] - yMean) * (ys[i] - yMean);
+                ssRes += (ys[i] - yHat) * (ys[i] - yHat);
+            }
+            if (ssTot > 0.0) {
+                const double r2 = 1.0 - ssRes / ssTot;
+                const double gamma = -slope;
+                powerLaw = r2 >= 0.70 && gamma >= 1.0 && gamma <= 5.0;
+            }
+        }
+    }
+    return heavyTail || powerLaw;
+}
+
+bool classify_social(const Csc& g) {
+    std::vector<uint32_t> outDeg(g.n), inDeg(g.n, 0);
+    for (uint32_t j = 0; j < g.n; ++j) outDeg[j] = g.degree(j);
+    for (uint32_t p = 0; p < g.nnz; ++p)
+        if (g.rows[p] < g.n) ++inDeg[g.rows[p]];
+    bool social = is_social_degree_distribution(inDeg) || is_social_degree_distribution(outDeg);
+    return social || (g.average_degree() > kSocialThreshold);
+}
+
+static void sort_columns(Csc& g) {
+#pragma omp parallel for schedule(dynamic, 2048)
+    for (int64_t j = 0; j < (int64_t)g.n; ++j)
+        std::sort(g.rows.begin() + g.col_ptrs[j], g.rows.begin() + g.col_ptrs[j + 1]);
+}
+
+Csc csc_read_mtx(const std::string& path, bool undirected, bool binary) {
+    std::ifstream file(path);
+    if (!file.is_open()) throw Error(BLEST_ERR_IO, "cannot open Matrix Market file: " + path);
+    while (file.peek() == '%') file.ignore(1 << 20, '\n');
+    uint32_t n = 0, n2 = 0;
+    uint64_t lines = 0;
+    if (!(file >> n >> n2 >> lines)) throw Error(BLEST_ERR_IO, "bad Matrix Market size line: " + path);
+    std::vector<std::vector<uint32_t>> adj(n);
+    uint64_t nnz = 0;
+    for (uint64_t it = 0; it < lines; ++it) {
+        uint64_t j, i;
+        double trash;
+        if (!(file >> j >> i)) throw Error(BLEST_ERR_IO, "truncated Matrix Market file: " + path);
+        if (!binary && !(file >> trash)) throw Error(BLEST_ERR_IO, "missing value in Matrix Market entry: " + path);
+        if (i == j) continue;
+        if (i == 0 || j == 0 || i > n || j > n) throw Error(BLEST_ERR_IO, "Matrix Market index out of range: " + path);
+        adj[j - 1].push_back((uint32_t)(i - 1));
+        ++nnz;
+        if (undirected) {
+            adj[i - 1].push_back((uint32_t)(j - 1));
+            ++nnz;
+        }
+    }
+    if (nnz > 0xFFFFFFFFull) throw Error(BLEST_ERR_UNSUPPORTED, "more than 2^32-1 non-zeros");
+    Csc g;
+    g.n = n;
+    g.nnz = (uint32_t)nnz;
+    g.col_ptrs.assign((size_t)n + 1, 0);
+    for (uint32_t j = 0; j < n; ++j) g.col_ptrs[j + 1] = g.col_ptrs[j] + (uint32_t)adj[j].size();
+    g.rows.resize(nnz);
+    for (uint32_t j = 0; j < n; ++j) std::copy(adj[j].begin(), adj[j].end(), g.rows.begin() + g.col_ptrs[j]);
+    sort_columns(g);
+    g.is_social = classify_social(g);
+    return g;
+}
+
+Csc csc_read_mtx_auto(const std::string& path) {
+    std::ifstream file(path);
+    if (!file.is_open()) throw Error(BLEST_ERR_IO, "cannot open Matrix Market file: " + path);
+    std::string banner;
+    std::getline(file, banner);
+    std::string lower = banner;
+    std::transform(lower.begin(), lower.end(), lower.begin(), ::tolower);
+    const bool binary = lower.find("pattern") != std::string::npos;
+    const bool undirected = lower.find("symmetric") != std::string::npos ||
+                            lower.find("hermitian") != std::string::npos;
+    file.close();
+    return csc_read_mtx(path, undirected, binary);
+}
+
+void csc_save_bin(const Csc& g, const std::string& path) {
+    std::ofstream out(path, std::ios::binary);
+    if (!out) throw Error(BLEST_ERR_IO, "cannot write " + path);
+    const uint8_t social = g.is_social ? 1 : 0;
+    out.write((const char*)&g.n, 4);
+    out.write((const char*)&g.nnz, 4);
+    out.write((const char*)&social, 1);
+    out.write((const char*)g.col_ptrs.data(), 4ull * (g.n + 1ull));
+    out.write((const char*)g.rows.data(), 4ull * g.nnz);
+    if (!out) throw Error(BLEST_ERR_IO, "short write to " + path);
+}
+
+Csc csc_load_bin(const std::string& path) {
+    std::ifstream in(path, std::ios::binary);
+    if (!in) throw Error(BLEST_ERR_IO, "cannot open " + path);
+    in.seekg(0, std::ios::end);
+    const uint64_t size = (uint64_t)in.tellg();
+    in.seekg(0);
+    Csc g;
+    uint8_t social = 0;
+    in.read((char*)&g.n, 4);
+    in.read((char*)&g.nnz, 4);
+    in.read((char*)&social, 1);
+    if (!in || size != 9ull + 4ull * (g.n + 1ull) + 4ull * g.nnz)
+        throw Error(BLEST_ERR_IO, "corrupt or truncated CSC cache: " + path);
+    g.is_social = social != 0;
+    g.col_ptrs.resize((size_t)g.n + 1);
+    g.rows.resize(g.nnz);
+    in.read((char*)g.col_ptrs.data(), 4ull * (g.n + 1ull));
+    in.read((char*)g.rows.data(), 4ull * g.nnz);
+    if (!in) throw Error(BLEST_ERR_IO, "short read from " + path);
+    if (g.col_ptrs[0] != 0 || g.col_ptrs[g.n] != g.nnz) throw Error(BLEST_ERR_IO, "inconsistent CSC cache: " + path);
+    for (uint32_t j = 0; j < g.n; ++j)
+        if (g.col_ptrs[j] > g.col_ptrs[j + 1]) throw Error(BLEST_ERR_IO, "inconsistent CSC cache: " + path);
+    for (uint32_t p = 0; p < g.nnz; ++p)
+        if (g.rows[p] >= g.n) throw Error(BLEST_ERR_IO, "row index out of range in CSC cache: " + path);
+    return g;
+}
+
+void ordering_save_bin(const std::vector<uint32_t>& inv, const std::string& path) {
+    std::ofstream out(path, std::ios::binary);
+    if (!out) throw Error(BLEST_ERR_IO, "cannot write " + path);
+    out.write((const char*)inv.data(), 4ull * inv.size());
+    if (!out) throw Error(BLEST_ERR_IO, "short write to " + path);
+}
+
+std::vector<uint32_t> ordering_load_bin(const std::string& path, uint32_t n) {
+    std::ifstream in(path, std::ios::binary);
+    if (!in) throw Error(BLEST_ERR_IO, "cannot open " + path);
+    in.seekg(0, std::ios::end);
+    if ((uint64_t)in.tellg() != 4ull * n) throw Error(BLEST_ERR_IO, "ordering cache size mismatch: " + path);
+    in.seekg(0);
+    std::vector<uint32_t> inv(n);
+    in.read((char*)inv.data(), 4ull * n);
+    if (!in) throw Error(BLEST_ERR_IO, "short read from " + path);
+    if (!permutation_check(inv, n)) throw Error(BLEST_ERR_IO, "ordering cache is not a permutation: " + path);
+    return inv;
+}
+
+Csc csc_transpose(const Csc& g) {
+    Csc t;
+    t.n = g.n;
+    t.nnz = g.nnz;
+    t.is_social = g.is_social;
+    t.col_ptrs.assign((size_t)g.n + 1, 0);
+    t.rows.resize(g.nnz);
+    for (uint32_t p = 0; p < g.nnz; ++p) ++t.col_ptrs[g.rows[p] + 1];
+    for (uint32_t i = 1; i <= g.n; ++i) t.col_ptrs[i] += t.col_ptrs[i - 1];
+    std::vector<uint32_t> cursor(t.col_ptrs.begin(), t.col_ptrs.end() - 1);
+    // Columns visited in increasing j, so every transposed list is sorted.
+    for (uint32_t j = 0; j < g.n; ++j)
+        for (uint32_t p = g.col_ptrs[j]; p < g.col_ptrs[j + 1]; ++p) t.rows[cursor[g.rows[p]]++] = j;
+    return t;
+}
+
+bool csc_check_symmetry(const Csc& g) {
+    for (uint32_t j = 0; j < g.n; ++j) {
+        for (uint32_t p = g.col_ptrs[j]; p < g.col_ptrs[j + 1]; ++p) {
+            const uint32_t i = g.rows[p];
+            if (i == j) continue;
+            const auto b = g.rows.begin() + g.col_ptrs[i], e = g.rows.begin() + g.col_ptrs[i + 1];
+            if (!std::binary_search(b, e, j)) return false;
+        }
+    }
+    return true;
+}
+
+Csc csc_symmetrize(const Csc& g) {
+    std::vector<std::vector<uint32_t>> cols(g.n);
+    for (uint32_t j = 0; j < g.n; ++j) {
+        for (uint32_t p = g.col_ptrs[j]; p < g.col_ptrs[j + 1]; ++p) {
+            const uint32_t i = g.rows[p];
+            cols[j].push_back(i);
+            if (i != j) cols[i].push_back(j);
+        }
+    }
+    Csc s;
+    s.n = g.n;
+    s.is_social = g.is_social;
+    s.col_ptrs.assign((size_t)g.n + 1, 0);
+    uint64_t nnz = 0;
+    for (uint32_t j = 0; j < g.n; ++j) {
+        auto& v = cols[j];
+        std::sort(v.begin(), v.end());
+        v.erase(std::unique(v.begin(), v.end()), v.end());
+        nnz += v.size();
+        s.col_ptrs[j + 1] = (uint32_t)nnz;
+    }
+    s.nnz = (uint32_t)nnz;
+    s.rows.resize(nnz);
+    for (uint32_t j = 0; j < g.n; ++j) std::copy(cols[j].begin(), cols[j].end(), s.rows.begin() + s.col_ptrs[j]);
+    return s;
+}
+
+bool permutation_check(const std::vector<uint32_t>& inv, uint32_t n) {
+    if (inv.size() != n) return false;
+    std::vector<uint8_t> seen(n, 0);
+    for (uint32_t v : inv) {
+        if (v >= n || seen[v]) return false;
+        seen[v] = 1;
+    }
+    return true;
+}
+
+void csc_apply_permutation(Csc& g, const std::vector<uint32_t>& inv) {
+    if (!permutation_check(inv, g.n)) throw Error(BLEST_ERR_INVALID_ARG, "Permutation check has failed.");
+    std::vector<uint32_t> ptrs((size_t)g.n + 1, 0);
+    for (uint32_t old = 0; old < g.n; ++old) ptrs[inv[old] + 1] = g.degree(old);
+    for (uint32_t j = 0; j < g.n; ++j) ptrs[j + 1] += ptrs[j];
+    std::vector<uint32_t> rows(g.nnz);
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int64_t old = 0; old < (int64_t)g.n; ++old) {
+        const uint32_t nc = inv[old];
+        uint32_t* dst = rows.data() + ptrs[nc];
+        const uint32_t b = g.col_ptrs[old], e = g.col_ptrs[old + 1];
+        for (uint32_t p = b; p < e; ++p) dst[p - b] = inv[g.rows[p]];
+        std::sort(dst, dst + (e - b));
+    }
+    g.col_ptrs.swap(ptrs);
+    g.rows.swap(rows);
+}
+
+Csc csc_from_undirected_edges(uint32_t n, uint64_t m, const EdgeFn& edge) {
+    std::vector<uint32_t> deg((size_t)n + 1, 0);
+#pragma omp parallel for schedule(static, 1 << 16)
+    for (int64_t e = 0; e < (int64_t)m; ++e) {
+        uint32_t u, v;
+        if (!edge((uint64_t)e, &u, &v) || u == v) continue;
+        __atomic_fetch_add(&deg[u], 1u, __ATOMIC_RELAXED);
+        __atomic_fetch_add(&deg[v], 1u, __ATOMIC_RELAXED);
+    }
+    std::vector<uint64_t> raw((size_t)n + 1, 0);
+    for (uint32_t j = 0; j < n; ++j) raw[j + 1] = raw[j] + deg[j];
+    const uint64_t total = raw[n];
+    std::vector<uint32_t> tmp(total);
+    std::vector<uint64_t> cursor(raw.begin(), raw.end() - 1);
+#pragma omp parallel for schedule(static, 1 << 16)
+    for (int64_t e = 0; e < (int64_t)m; ++e) {
+        uint32_t u, v;
+        if (!edge((uint64_t)e, &u, &v) || u == v) continue;
+        tmp[__atomic_fetch_add(&cursor[u], 1ull, __ATOMIC_RELAXED)] = v;
+        tmp[__atomic_fetch_add(&cursor[v], 1ull, __ATOMIC_RELAXED)] = u;
+    }
+    cursor.clear();
+    cursor.shrink_to_fit();
+    // Sort + unique each column; the column's unique count goes to deg.
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int64_t j = 0; j < (int64_t)n; ++j) {
+        uint32_t* b = tmp.data() + raw[j];
+        uint32_t* e = tmp.data() + raw[j + 1];
+        std::sort(b, e);
+        deg[j] = (uint32_t)(std::unique(b, e) - b);
+    }
+    uint64_t nnz = 0;
+    for (uint32_t j = 0; j < n; ++j) nnz += deg[j];
+    if (nnz > 0xFFFFFFFFull) throw Error(BLEST_ERR_UNSUPPORTED, "more than 2^32-1 non-zeros");
+    Csc g;
+    g.n = n;
+    g.nnz = (uint32_t)nnz;
+    g.col_ptrs.assign((size_t)n + 1, 0);
+    for (uint32_t j = 0; j < n; ++j) g.col_ptrs[j + 1] = g.col_ptrs[j] + deg[j];
+    g.rows.resize(nnz);
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int64_t j = 0; j < (int64_t)n; ++j)
+        std::memcpy(g.rows.data() + g.col_ptrs[j], tmp.data() + raw[j], 4ull * deg[j]);
+    g.is_social = classify_social(g);
+    return g;
+}
+
+Csc csc_from_arrays(uint32_t n, const uint32_t* col_ptrs, const uint32_t* rows) {
+    if (col_ptrs[0] != 0) throw Error(BLEST_ERR_INVALID_ARG, "col_ptrs[0] must be 0");
+    for (uint32_t j = 0; j < n; ++j)
+        if (col_ptrs[j] > col_ptrs[j + 1]) throw Error(BLEST_ERR_INVALID_ARG, "col_ptrs must be non-decreasing");
+    Csc g;
+    g.n = n;
+    g.nnz = col_ptrs[n];
+    g.col_ptrs.assign(col_ptrs, col_ptrs + n + 1);
+    g.rows.assign(rows, rows + g.nnz);
+    for (uint32_t p = 0; p < g.nnz; ++p)
+        if (g.rows[p] >= n) throw Error(BLEST_ERR_INVALID_ARG, "row index out of range");
+    sort_columns(g);
+    g.is_social = classify_social(g);
+    return g;
+}
+
+std::vector<uint32_t> seeded_permutation(uint32_t n, uint64_t seed) {
+    std::vector<uint32_t> perm(n);
+    for (uint32_t i = 0; i < n; ++i) perm[i] = i;
+    SeqRng rng(seed ^ 0x5EEDBEEFCAFEF00Dull);
+    for (uint32_t i = n; i > 1; --i) {
+        const uint32_t j = (uint32_t)rng.below(i);
+        std::swap(perm[i - 1], perm[j]);
+    }
+    return perm;
+}
+
+std::vector<uint32_t> sample_sources(const Csc& g, uint32_t k, uint64_t seed) {
+    std::vector<uint32_t> cand;
+    for (uint32_t v = 0; v < g.n; ++v)
+        if (g.degree(v) >= 1) cand.push_back(v);
+    SeqRng rng(seed ^ 0x50C5A3B1E5ull);
+    const uint32_t take = std::min<uint32_t>(k, (uint32_t)cand.size());
+    for (uint32_t i = 0; i < take; ++i) {
+        const uint32_t j = i + (uint32_t)rng.below(cand.size() - i);
+        std::swap(cand[i], cand[j]);
+    }
+    cand.resize(take);
+    return cand;
+}
+
+}  // namespace blest

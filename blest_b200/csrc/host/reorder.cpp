@@ -1,0 +1,270 @@
+// Vertex orderings applied before BVSS compression. The windowed Jaccard
+// and RCM orders restate the reference's greedy rules exactly (same
+// candidate, same tie-break, same floating-point score), so the BVSS built
+// from them is byte-identical to the reference's; only the bookkeeping is
+// cheaper (see the notes on each function).
+#include "reorder.hpp"
+
+#include <omp.h>
+
+#include <algorithm>
+#include <numeric>
+
+#include "blest.h"
+
+namespace blest {
+
+std::vector<uint32_t> order_natural(const Csc& g) {
+    std::vector<uint32_t> inv(g.n);
+    std::iota(inv.begin(), inv.end(), 0u);
+    return inv;
+}
+
+std::vector<uint32_t> order_random(const Csc& g, uint64_t seed) {
+    // CSC.cuh:535-554 shuffles with std::random_device; seeded here.
+    const std::vector<uint32_t> perm = seeded_permutation(g.n, seed);
+    std::vector<uint32_t> inv(g.n);
+    for (uint32_t i = 0; i < g.n; ++i) inv[perm[i]] = i;
+    return inv;
+}
+
+std::vector<uint32_t> order_degree(const Csc& g, bool ascending) {
+    // CSC.cuh:968-992: sort by degree, ties by id.
+    std::vector<uint32_t> ids(g.n);
+    std::iota(ids.begin(), ids.end(), 0u);
+    std::sort(ids.begin(), ids.end(), [&](uint32_t x, uint32_t y) {
+        const uint32_t dx = g.degree(x), dy = g.degree(y);
+        if (dx != dy) return ascending ? dx < dy : dx > dy;
+        return x < y;
+    });
+    std::vector<uint32_t> inv(g.n);
+    for (uint32_t i = 0; i < g.n; ++i) inv[ids[i]] = i;
+    return inv;
+}
+
+// Windowed Jaccard ordering, CSC.cuh:717-920.
+// Columns are split into windows of `window` consecutive ids; inside a
+// window, slice sets of `slice_size` new ids are filled greedily: the first
+// column of each slice set is the unplaced column of largest degree (ties:
+// largest id, from the `deg >= max` scan at CSC.cuh:768-785); each next
+// column is the queued candidate with the best Jaccard score
+// |rows(set) & rows(c)| / |rows(set) | rows(c)| (first in queue order on
+// ties, swap-removed from the queue); with an empty queue the next column
+// is again the largest-degree unplaced one.
+// Differences in bookkeeping only: the largest-degree scan walks a
+// (degree desc, id desc) order once per window instead of rescanning the
+// window; the first in-window position of a transposed row is found by
+// binary search instead of a linear scan plus a per-window O(n) cache
+// reset; intersection counts are cleared by a touched list. None of these
+// change which column is chosen.
+std::vector<uint32_t> order_jaccard_window(const Csc& g, uint32_t slice_size, uint32_t window, int threads) {
+    if (slice_size == 0 || window == 0 || window % slice_size != 0)
+        throw Error(BLEST_ERR_INVALID_ARG, "Jaccard window must be a positive multiple of the slice size");
+    const uint32_t n = g.n;
+    std::vector<uint32_t> inv(n, 0);
+    if (n == 0) return inv;
+    const Csc t = csc_transpose(g);
+    const uint32_t* ptrs = t.col_ptrs.data();
+    const uint32_t* ids = t.rows.data();
+    const uint32_t* cp = g.col_ptrs.data();
+    const uint32_t* rows = g.rows.data();
+    const uint32_t noWindows = (uint32_t)((n + (uint64_t)window - 1) / window);
+    int nt = threads > 0 ? threads : omp_get_max_threads();
+    nt = std::max(1, std::min<int>(nt, (int)noWindows));
+
+#pragma omp parallel num_threads(nt)
+    {
+        const uint32_t W = std::min(window, n);
+        std::vector<uint8_t> cmark(W);
+        std::vector<uint32_t> inter(W, 0);
+        std::vector<uint32_t> touched;
+        touched.reserve(W);
+        std::vector<uint32_t> queue(W);
+        std::vector<uint32_t> byDeg(W);
+        std::vector<uint32_t> rmark(n, 0);
+        uint32_t epoch = 1;
+
+#pragma omp for schedule(dynamic)
+        for (int64_t w = 0; w < (int64_t)noWindows; ++w) {
+            const uint32_t ws = (uint32_t)w * window;
+            const uint32_t we = (uint32_t)std::min<uint64_t>((uint64_t)ws + window, n);
+            const uint32_t len = we - ws;
+            std::fill(cmark.begin(), cmark.begin() + len, 0);
+            for (uint32_t i = 0; i < len; ++i) byDeg[i] = ws + i;
+            std::sort(byDeg.begin(), byDeg.begin() + len, [&](uint32_t x, uint32_t y) {
+                const uint32_t dx = cp[x + 1] - cp[x], dy = cp[y + 1] - cp[y];
+                if (dx != dy) return dx > dy;
+                return x > y;
+            });
+            uint32_t degCursor = 0;
+            auto selectSingleton = [&](uint32_t& col) -> bool {
+                while (degCursor < len && cmark[byDeg[degCursor] - ws]) ++degCursor;
+                if (degCursor == len) return false;
+                col = byDeg[degCursor];
+                return true;
+            };
+            uint32_t qsize = 0;
+            uint32_t unionSize = 0;
+            // Count, for every unplaced in-window column c sharing row r,
+            // one more common row (CSC.cuh:796-826 / 858-888).
+            auto scanRow = [&](uint32_t r) {
+                const uint32_t* b = ids + ptrs[r];
+                const uint32_t* e = ids + ptrs[r + 1];
+                for (const uint32_t* p = std::lower_bound(b, e, ws); p < e; ++p) {
+                    const uint32_t c = *p;
+                    if (c >= we) break;
+                    if (!cmark[c - ws]) {
+                        if (inter[c - ws] == 0) {
+                            queue[qsize++] = c;
+                            touched.push_back(c - ws);
+                        }
+                        ++inter[c - ws];
+                    }
+                }
+            };
+            const uint32_t noSets = (len + slice_size - 1) / slice_size;
+            for (uint32_t s = 0; s < noSets; ++s) {
+                for (uint32_t x : touched) inter[x] = 0;
+                touched.clear();
+                qsize = 0;
+                const uint32_t sliceStart = ws + s * slice_size;
+                const uint32_t sliceEnd = std::min(sliceStart + slice_size, we);
+                ++epoch;
+                unionSize = 0;
+                uint32_t single = 0;
+                selectSingleton(single);
+                cmark[single - ws] = 1;
+                for (uint32_t p = cp[single]; p < cp[single + 1]; ++p) {
+                    const uint32_t r = rows[p];
+                    rmark[r] = epoch;
+                    ++unionSize;
+                    scanRow(r);
+                }
+                inv[single] = sliceStart;
+                for (uint32_t newCol = sliceStart + 1; newCol < sliceEnd; ++newCol) {
+                    uint32_t best;
+                    if (qsize == 0) {
+                        if (!selectSingleton(best)) break;
+                    } else {
+                        uint32_t bi = 0;
+                        double bestVal = -1;
+                        for (uint32_t q = 0; q < qsize; ++q) {
+                            const uint32_t j = queue[q];
+                            const uint32_t in = inter[j - ws];
+                            const uint32_t deg = cp[j + 1] - cp[j];
+                            const uint32_t uni = unionSize + deg - in;
+                            const double val = (uni == 0) ? 1.0 : (double)in / uni;
+                            if (val > bestVal) {
+                                bi = q;
+                                bestVal = val;
+                            }
+                        }
+                        best = queue[bi];
+                        queue[bi] = queue[qsize - 1];
+                        --qsize;
+                    }
+                    cmark[best - ws] = 1;
+                    for (uint32_t p = cp[best]; p < cp[best + 1]; ++p) {
+                        const uint32_t r = rows[p];
+                        if (rmark[r] != epoch) {
+                            rmark[r] = epoch;
+                            ++unionSize;
+                            scanRow(r);
+                        }
+                    }
+                    inv[best] = newCol;
+                }
+            }
+        }
+    }
+    return inv;
+}
+
+// Ordering of CSC::rcm (CSC.cuh:1059-1142) with the pseudo-peripheral
+// start of CSC.cuh:994-1057. As in the reference the BFS order is used
+// without reversal (inversePermutation[u] = position in the Cuthill-McKee
+// queue), neighbours are ordered by std::sort on ascending degree (the
+// same unstable sort on the same input gives the same order), and the
+// restart vertex is drawn from the last BFS level with the C library
+// rand() sequence, reproduced by GlibcRand from `rand_seed` (1 = the
+// reference's never-seeded state). The per-call O(n) marker allocation of
+// the reference is replaced by one stamped marker array.
+std::vector<uint32_t> order_rcm(const Csc& g0, uint32_t rand_seed) {
+    const Csc* gp = &g0;
+    Csc sym;
+    if (!csc_check_symmetry(g0)) {
+        sym = csc_symmetrize(g0);
+        gp = &sym;
+    }
+    const Csc& g = *gp;
+    const uint32_t n = g.n;
+    const uint32_t* ptrs = g.col_ptrs.data();
+    const uint32_t* inds = g.rows.data();
+    std::vector<uint32_t> inv(n, 0), degrees(n), visited(n, 0), q(n), nbrs(n), stamp(n, 0);
+    for (uint32_t i = 0; i < n; ++i) degrees[i] = ptrs[i + 1] - ptrs[i];
+    GlibcRand rng(rand_seed);
+    uint32_t marker = 1;
+
+    auto pseudoPeripheral = [&](uint32_t startNode) -> uint32_t {
+        uint32_t maxLevel = 0, trial = 0;
+        while (trial < 10) {
+            ++marker;
+            q[0] = startNode;
+            stamp[startNode] = marker;
+            uint32_t qe = 1, qs = 0, levelStart = 0, levelEnd = qe, levelid = 1;
+            while (qs < qe) {
+                const uint32_t u = q[qs++];
+                for (uint32_t p = ptrs[u]; p < ptrs[u + 1]; ++p) {
+                    const uint32_t v = inds[p];
+                    if (stamp[v] != marker) {
+                        stamp[v] = marker;
+                        q[qe++] = v;
+                    }
+                }
+                if (qs == levelEnd && qs < qe) {
+                    levelStart = qs;
+                    levelEnd = qe;
+                    levelid++;
+                }
+            }
+            if (levelid == maxLevel) trial++;
+            else trial = 0;
+            maxLevel = levelid;
+            startNode = q[levelStart + ((uint32_t)rng() % (levelEnd - levelStart))];
+        }
+        return startNode;
+    };
+
+    auto compAsc = [&](uint32_t a, uint32_t b) { return degrees[a] < degrees[b]; };
+    uint32_t permuted = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (visited[i] == 1) continue;
+        const uint32_t start = pseudoPeripheral(i);
+        uint32_t qs = 0, qe = 0;
+        q[qe++] = start;
+        visited[start] = 1;
+        while (qs < qe) {
+            const uint32_t u = q[qs++];
+            inv[u] = permuted++;
+            uint32_t k = 0;
+            for (uint32_t p = ptrs[u]; p < ptrs[u + 1]; ++p) {
+                const uint32_t v = inds[p];
+                if (visited[v] == 0) {
+                    nbrs[k++] = v;
+                    visited[v] = 1;
+                }
+            }
+            std::sort(nbrs.begin(), nbrs.begin() + k, compAsc);
+            for (uint32_t x = 0; x < k; ++x) q[qe++] = nbrs[x];
+        }
+    }
+    return inv;
+}
+
+}  // namespace blest
+
+namespace blest {
+std::vector<uint32_t> order_gorder(const Csc&, uint32_t) {
+    throw Error(BLEST_ERR_UNSUPPORTED, "Gorder ordering is not built yet");
+}
+}  // namespace blest
