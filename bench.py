@@ -40,6 +40,7 @@ WORKLOADS = {
     "rmat16": ("bfs", ("rmat", 16, 16), "jaccard", 65536, 64,
                "RMAT scale 16 ef 16, Jaccard window 65536, 64 seeded sources"),
     "rmat20": ("bfs", ("rmat", 20, 16), "jaccard", 65536, 64, "RMAT scale 20 ef 16, Jaccard window 65536"),
+    "rmat22": ("bfs", ("rmat", 22, 16), "jaccard", 65536, 64, "RMAT scale 22 ef 16, Jaccard window 65536"),
     "grid4096": ("bfs", ("grid", 4096, 4096), "rcm", 0, 32,
                  "2D 4096x4096 grid, 5% edges deleted, 0.1% shortcuts, RCM, 32 seeded sources"),
     "er25": ("bfs", ("er", 25, 32), "rcm", 0, 32, "Erdos-Renyi 2^25 vertices avg degree 32, RCM, 32 sources"),

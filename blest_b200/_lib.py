@@ -36,6 +36,7 @@ ERR_ADMISSION = 9
 ERR_DEVICE_INDEX = 10
 ERR_BUSY = 11
 UNREACHED = 0xFFFFFFFF
+NOALLOC_MAX_VERTICES = 1 << 20
 MEM_HOST = 0
 MEM_DEVICE = 1
 
@@ -88,6 +89,12 @@ class BfsStats(C.Structure):
 
 class CcStats(C.Structure):
     _fields_ = [("time", f64), ("no_components", u32), ("iterations", u32)]
+
+
+class DeviceGraphView(C.Structure):
+    _fields_ = [("n", u32), ("no_real_slice_sets", u32), ("no_slices", u64), ("nnz", u32),
+                ("slice_set_ptrs", vp), ("real_ptrs", vp), ("row_ids", vp), ("masks", vp),
+                ("csr_ptrs", vp), ("csr_ids", vp)]
 
 
 class MbfsParams(C.Structure):
@@ -149,6 +156,7 @@ _SIGS = {
     "blest_bfs": [vp, u32, vp, vp, i32, P(BfsParams), P(BfsStats)],
     "blest_bfs_ws": [vp, u32, vp, vp, i32, P(BfsParams), vp, i32, P(BfsStats)],
     "blest_workspace_sync": [vp, P(BfsStats)],
+    "blest_bfs_noalloc": [P(DeviceGraphView), u32, vp, vp, vp, P(BfsStats)],
     "blest_cc": [vp, vp, i32, P(CcStats)],
     "blest_cc_ws": [vp, vp, i32, vp, P(CcStats)],
     "blest_cc_relabel_dense": [P(u32), u32, P(u32), P(u32)],

@@ -20,10 +20,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
+#include <mutex>
+#include <string>
 
 #include "common.cuh"
 #include "runtime.hpp"
 #include "../host/common.hpp"
+#include "../host/errors.hpp"
 
 namespace blest {
 namespace dev {
@@ -457,3 +461,143 @@ void launch_bfs(const blest_graph* g, Workspace& w, uint32_t src, uint32_t* leve
 }
 
 }  // namespace blest
+
+// ---------------------------------------------------------------------------
+// Allocation-free BFS (blest_bfs_noalloc). Some callers cannot call
+// cudaMalloc: a host application that owns all device memory through its
+// own pool and forbids other allocations, a latency-critical path where
+// cudaMalloc/cudaFree may synchronise the device, or a plugin that must not
+// change the process's memory footprint per call. For them this entry
+// point keeps its scratch (visited/frontier bitmaps, the rset tile table,
+// the rset queue and the run counters) in one file-scope device array of
+// fixed size, sized for graphs of at most kNoAllocMaxVertices vertices.
+// Every GPU that loads this library holds that array (about 9 MiB) until
+// the process exits. The caller passes the graph and the outputs in its own
+// device memory.
+namespace blest {
+namespace {
+
+constexpr uint32_t kNoAllocMaxVertices = BLEST_NOALLOC_MAX_VERTICES;
+constexpr uint32_t kNoAllocWords = kNoAllocMaxVertices / 32;          // words per bitmap
+constexpr uint32_t kNoAllocRsets = kNoAllocMaxVertices / 8;           // real slice sets
+constexpr uint32_t kNoAllocQueue = kNoAllocRsets * 8 + 64;            // rset queue entries
+constexpr size_t kNaVisited = 0;
+constexpr size_t kNaFrontier = kNaVisited + 4ull * kNoAllocWords;     // 3 bitmaps
+constexpr size_t kNaRsetTile = kNaFrontier + 3 * 4ull * kNoAllocWords;
+constexpr size_t kNaQRset = kNaRsetTile + 4ull * (kNoAllocRsets + 64);
+constexpr size_t kNaQOff = kNaQRset + 4ull * kNoAllocQueue;
+constexpr size_t kNaCounters = (kNaQOff + 4ull * kNoAllocQueue + 255) & ~size_t(255);
+constexpr size_t kNoAllocBytes = kNaCounters + ((sizeof(dev::RunCounters) + 255) & ~size_t(255));
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex[kNoAllocMaxDevices];
+unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+__global__ void noalloc_rset_tile_kernel(const uint64_t* ssp, const uint32_t* real_ptrs, uint32_t R, uint32_t* out) {
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r <= R; r += gridDim.x * blockDim.x)
+        out[r] = (uint32_t)(ssp[real_ptrs[r]] / 4);
+}
+
+template <bool PARENTS>
+void noalloc_launch(const dev::BfsArgs& a, int sms, cudaStream_t s) {
+    auto kern = dev::bfs_persistent_kernel<false, false, PARENTS>;
+    int maxBlocks = 0;
+    BLEST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxBlocks, kern, 512, 0));
+    if (maxBlocks < 1) throw Error(BLEST_ERR_CUDA, "BFS kernel cannot be resident");
+    dev::bfs_init_kernel<<<sms * 4, 512, 0, s>>>(a);
+    BLEST_CUDA(cudaGetLastError());
+    dev::bfs_seed_kernel<false><<<1, 1, 0, s>>>(a);
+    BLEST_CUDA(cudaGetLastError());
+    void* kargs[] = {(void*)&a};
+    BLEST_CUDA(cudaLaunchCooperativeKernel((void*)kern, maxBlocks * sms, 512, kargs, 0, s));
+}
+
+}  // namespace
+}  // namespace blest
+
+extern "C" int blest_bfs_noalloc(const blest_device_graph_view* g, uint32_t source, uint32_t* levels_out,
+                                 uint32_t* parents_out, void* stream, blest_bfs_stats* stats) {
+    using namespace blest;
+    return guarded([&] {
+        require(g && levels_out, "null argument");
+        if (g->n == 0 || source >= g->n) throw Error(BLEST_ERR_INVALID_ARG, "source vertex out of range");
+        if (g->n > kNoAllocMaxVertices)
+            throw Error(BLEST_ERR_UNSUPPORTED, "blest_bfs_noalloc handles at most " +
+                                                   std::to_string(kNoAllocMaxVertices) + " vertices; graph has " +
+                                                   std::to_string(g->n) + " (use blest_bfs)");
+        require(g->no_real_slice_sets == (g->n + 7) / 8, "no_real_slice_sets != ceil(n/8)");
+        require(g->no_slices % 4 == 0 && g->no_slices / 4 < 0xFFFFFFFFull, "bad slice count");
+        require(g->slice_set_ptrs && g->real_ptrs && g->csr_ptrs && (g->no_slices == 0 || (g->row_ids && g->masks)) &&
+                    (g->nnz == 0 || g->csr_ids),
+                "null graph array");
+        require(((uintptr_t)g->row_ids & 15) == 0, "row_ids must be 16-byte aligned");
+        int device = 0;
+        BLEST_CUDA(cudaGetDevice(&device));
+        require(device >= 0 && device < kNoAllocMaxDevices, "device ordinal out of range");
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex[device]);
+        // One-time set-up per device (this device current): the device
+        // address of the scratch array.
+        if (!g_noalloc_ptr[device]) {
+            void* p = nullptr;
+            BLEST_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+            g_noalloc_ptr[device] = (unsigned char*)p;
+        }
+        unsigned char* base = g_noalloc_ptr[device];
+        int sms = 0;
+        BLEST_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+        cudaStream_t s = (cudaStream_t)stream;
+
+        dev::BfsArgs a{};
+        a.g.n = g->n;
+        a.g.no_real = g->no_real_slice_sets;
+        a.g.nnz = g->nnz;
+        a.g.no_slices = g->no_slices;
+        a.g.degree_total = g->nnz;
+        a.g.slice_set_ptrs = g->slice_set_ptrs;
+        a.g.real_ptrs = g->real_ptrs;
+        a.g.row4 = (const uint4*)g->row_ids;
+        a.g.masks = g->masks;
+        a.g.rset_tile = (const uint32_t*)(base + kNaRsetTile);
+        a.g.csr_ptrs = g->csr_ptrs;
+        a.g.csr_ids = g->csr_ids;
+        a.levels = levels_out;
+        a.parents = parents_out;
+        a.visited = (uint32_t*)(base + kNaVisited);
+        a.frontier0 = (uint32_t*)(base + kNaFrontier);
+        a.frontier1 = a.frontier0 + kNoAllocWords;
+        a.frontier2 = a.frontier1 + kNoAllocWords;
+        a.q_rset = (uint32_t*)(base + kNaQRset);
+        a.q_off = (uint32_t*)(base + kNaQOff);
+        a.ctr = (dev::RunCounters*)(base + kNaCounters);
+        a.words = ((g->n + 31) / 32 + 3) & ~3u;
+        a.src = source;
+        a.direction = BLEST_DIR_AUTO;
+        a.alpha = 14.0f;
+        a.beta = 24.0f;
+
+        const auto t0 = std::chrono::steady_clock::now();
+        noalloc_rset_tile_kernel<<<sms, 256, 0, s>>>(g->slice_set_ptrs, g->real_ptrs, g->no_real_slice_sets,
+                                                     (uint32_t*)(base + kNaRsetTile));
+        BLEST_CUDA(cudaGetLastError());
+        if (parents_out) noalloc_launch<true>(a, sms, s);
+        else noalloc_launch<false>(a, sms, s);
+        dev::RunCounters c;
+        BLEST_CUDA(cudaMemcpyAsync(&c, a.ctr, sizeof(c), cudaMemcpyDeviceToHost, s));
+        BLEST_CUDA(cudaStreamSynchronize(s));
+        const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (c.error)
+            throw Error((int)c.error, c.error == BLEST_ERR_BARRIER_TIMEOUT ? "device grid barrier timed out"
+                                                                          : "device reported an out-of-range index");
+        if (stats) {
+            stats->time = secs;
+            stats->source_vertex = source;
+            stats->total_levels = c.levels;
+            stats->no_visited = (uint32_t)c.discovered;
+            stats->push_levels = c.push_levels;
+            stats->pull_levels = c.pull_levels;
+            stats->reached_degree_sum = c.degree;
+        }
+    });
+}

@@ -258,6 +258,42 @@ int blest_bfs_ws(blest_workspace* ws, uint32_t source, uint32_t* levels_out, uin
                  const blest_bfs_params* params, void* stream, int async, blest_bfs_stats* stats);
 int blest_workspace_sync(blest_workspace* ws, blest_bfs_stats* stats);
 
+/* ---- allocation-free single-source BFS ------------------------------------
+ * This entry point has no counterpart in the reference.
+ * It is for callers that cannot call cudaMalloc: an application that owns
+ * all device memory through its own pool and forbids other allocations, a
+ * latency-critical path where cudaMalloc/cudaFree may synchronise the
+ * device, or a plugin that must not grow the process's memory per call.
+ * It allocates nothing: its scratch (frontier bitmaps, rset queue,
+ * counters) is one fixed device array inside the library, sized for graphs
+ * of at most BLEST_NOALLOC_MAX_VERTICES vertices (about 9 MiB, held on
+ * every GPU that loads the library until the process exits); larger graphs
+ * are rejected with BLEST_ERR_UNSUPPORTED. The caller passes the graph
+ * (a valid BVSS and its pull CSR, e.g. as built by blest_bvss_build and
+ * blest_csc_transpose, copied into its own device memory) and device
+ * output buffers. The first call on a device looks up the scratch array's
+ * device address (with that device current); make that first call before
+ * any stream capture. All calls on a device share the one scratch array,
+ * so calls whose GPU work overlapped would race: this function serialises
+ * callers per device and returns only when its work on `stream` is done.
+ * Levels (and parents, if non-NULL) are identical to blest_bfs's; stats
+ * time is host wall time of the call. */
+#define BLEST_NOALLOC_MAX_VERTICES (1u << 20)
+typedef struct blest_device_graph_view {
+    uint32_t n;
+    uint32_t no_real_slice_sets;       /* ceil(n / 8) */
+    uint64_t no_slices;
+    uint32_t nnz;                      /* CSR entries */
+    const uint64_t* slice_set_ptrs;    /* device [V + 1] */
+    const uint32_t* real_ptrs;         /* device [R + 1] */
+    const uint32_t* row_ids;           /* device [S], 16-byte aligned */
+    const uint32_t* masks;             /* device [S / 4] */
+    const uint32_t* csr_ptrs;          /* device [n + 1] */
+    const uint32_t* csr_ids;           /* device [nnz] */
+} blest_device_graph_view;
+int blest_bfs_noalloc(const blest_device_graph_view* g, uint32_t source, uint32_t* levels_out,
+                      uint32_t* parents_out, void* stream, blest_bfs_stats* stats);
+
 /* ---- connected components ------------------------------------------------ */
 /* Mirrors CCResult (CC/CCKernel.cuh:21-26). */
 typedef struct blest_cc_stats {
