@@ -79,7 +79,12 @@ class GraphInfo(C.Structure):
 
 class BfsParams(C.Structure):
     _fields_ = [("direction", i32), ("slice_test", i32), ("alpha", f64), ("beta", f64),
-                ("blocks_per_sm", i32), ("threads_per_block", i32)]
+                ("blocks_per_sm", i32), ("threads_per_block", i32), ("trace", i32)]
+
+
+class LevelTrace(C.Structure):
+    _fields_ = [("start_ns", u64), ("level", u32), ("direction", u32), ("frontier", u64), ("work_units", u64),
+                ("longest_scan", u64)]
 
 
 class BfsStats(C.Structure):
@@ -156,6 +161,8 @@ _SIGS = {
     "blest_bfs": [vp, u32, vp, vp, i32, P(BfsParams), P(BfsStats)],
     "blest_bfs_ws": [vp, u32, vp, vp, i32, P(BfsParams), vp, i32, P(BfsStats)],
     "blest_workspace_sync": [vp, P(BfsStats)],
+    "blest_workspace_trace": [vp, P(LevelTrace), u32, P(u32)],
+    "blest_graph_default_workspace": [vp, P(vp)],
     "blest_bfs_noalloc": [P(DeviceGraphView), u32, vp, vp, vp, P(BfsStats)],
     "blest_cc": [vp, vp, i32, P(CcStats)],
     "blest_cc_ws": [vp, vp, i32, vp, P(CcStats)],

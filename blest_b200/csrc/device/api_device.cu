@@ -113,6 +113,16 @@ int g_device = -1;
 
 }  // namespace
 
+void summary_geometry(uint32_t words, uint32_t& shift, uint32_t& sum_words) {
+    shift = 0;
+    for (;;) {
+        const uint64_t bits = ((uint64_t)words + (1ull << shift) - 1) >> shift;
+        sum_words = (uint32_t)((bits + 31) / 32);
+        if (4ull * sum_words <= kSummaryMaxBytes) return;
+        ++shift;
+    }
+}
+
 void workspace_alloc(const blest_graph* g, Workspace& w) {
     const uint32_t n = g->d.n;
     w.words = (((n + 31) / 32) + 3) & ~3u;
@@ -129,6 +139,11 @@ void workspace_alloc(const blest_graph* g, Workspace& w) {
     alloc((void**)&w.levels, 4ull * n);
     alloc((void**)&w.parents, 4ull * n);
     alloc((void**)&w.labels_old, 4ull * n);
+    alloc((void**)&w.trace, sizeof(blest_level_trace) * BLEST_TRACE_CAPACITY);
+    summary_geometry(w.words, w.sum_shift, w.sum_words);
+    for (int i = 0; i < 3; ++i) alloc((void**)&w.summary[i], 4ull * w.sum_words);
+    w.heavy_cap = g->d.nnz / 1024 + 64;
+    alloc((void**)&w.heavy, sizeof(uint4) * w.heavy_cap);
     BLEST_CUDA(cudaMallocHost((void**)&w.host_counters, sizeof(dev::RunCounters)));
     BLEST_CUDA(cudaEventCreate(&w.ev_start));
     BLEST_CUDA(cudaEventCreate(&w.ev_stop));
@@ -143,6 +158,9 @@ void workspace_free(Workspace& w) {
     cudaFree(w.levels);
     cudaFree(w.parents);
     cudaFree(w.labels_old);
+    cudaFree(w.trace);
+    for (auto& x : w.summary) cudaFree(x);
+    cudaFree(w.heavy);
     if (w.host_counters) cudaFreeHost(w.host_counters);
     if (w.ev_start) cudaEventDestroy(w.ev_start);
     if (w.ev_stop) cudaEventDestroy(w.ev_stop);
@@ -241,7 +259,28 @@ int blest_graph_create(const blest_bvss_view* bvss, const blest_csr_view* csr, b
         d.masks = blest::upload(g, bvss->masks, bvss->no_slices / 4);
         d.rset_tile = blest::upload(g, rsetTile.data(), rsetTile.size());
         d.csr_ptrs = blest::upload(g, csr->row_ptrs, (size_t)csr->n + 1);
-        d.csr_ids = blest::upload(g, csr->col_ids, csr->nnz);
+        {
+            // Pull order: each vertex's in-neighbours by descending degree
+            // (ties by id). High-degree vertices join the frontier first in
+            // skewed graphs, so the bottom-up scan, which stops at the first
+            // frontier neighbour, stops sooner. Levels do not depend on the
+            // order; only which valid parent is recorded does.
+            std::vector<uint32_t> ids(csr->col_ids, csr->col_ids + csr->nnz);
+            const uint32_t* rp = csr->row_ptrs;
+#pragma omp parallel for schedule(dynamic, 1024)
+            for (int64_t u = 0; u < (int64_t)csr->n; ++u) {
+                std::stable_sort(ids.begin() + rp[u], ids.begin() + rp[u + 1], [rp](uint32_t x, uint32_t y) {
+                    return rp[x + 1] - rp[x] > rp[y + 1] - rp[y];
+                });
+            }
+            d.csr_ids = blest::upload(g, ids.data(), ids.size());
+        }
+        {
+            std::vector<uint32_t> hasIn(((size_t)csr->n + 31) / 32 + 4, 0u);
+            for (uint32_t u = 0; u < csr->n; ++u)
+                if (csr->row_ptrs[u + 1] > csr->row_ptrs[u]) hasIn[u >> 5] |= 1u << (u & 31);
+            d.has_in = blest::upload(g, hasIn.data(), hasIn.size());
+        }
         g->undirected_edges = csr->nnz / 2;
         BLEST_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
         g->owns_stream = true;
@@ -360,6 +399,24 @@ int blest_workspace_sync(blest_workspace* ws, blest_bfs_stats* stats) {
         float ms = 0;
         BLEST_CUDA(cudaEventElapsedTime(&ms, ws->w.ev_start, ws->w.ev_stop));
         fill_bfs_stats(ws->w, ws->pending_src, ms, stats);
+    });
+}
+
+int blest_workspace_trace(blest_workspace* ws, blest_level_trace* out, uint32_t max, uint32_t* count) {
+    return guarded([&] {
+        blest::require(ws && out && count, "null argument");
+        BLEST_CUDA(cudaSetDevice(ws->g->device));
+        const uint32_t levels = ws->w.host_counters->levels + 1;  // + end record
+        const uint32_t k = std::min<uint32_t>(std::min<uint32_t>(levels, max), BLEST_TRACE_CAPACITY);
+        BLEST_CUDA(cudaMemcpy(out, ws->w.trace, sizeof(blest_level_trace) * k, cudaMemcpyDeviceToHost));
+        *count = k;
+    });
+}
+
+int blest_graph_default_workspace(blest_graph* g, blest_workspace** out) {
+    return guarded([&] {
+        blest::require(g && out, "null argument");
+        *out = g->default_ws;
     });
 }
 

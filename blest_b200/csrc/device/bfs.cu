@@ -48,7 +48,36 @@ struct BfsArgs {
     int direction;
     float alpha;
     float beta;
+    blest_level_trace* trace;  // optional per-level records
+    // Frontier summary per level (1 bit per 2^sum_shift frontier words),
+    // staged in shared memory by the pull phase to skip empty words.
+    uint32_t* summary0;
+    uint32_t* summary1;
+    uint32_t* summary2;
+    uint32_t sum_shift;
+    uint32_t sum_words;
+    // Pull: unvisited vertices whose remaining list is longer than
+    // heavy_min are scanned by all warps in kHeavyChunk pieces after a
+    // mid-level barrier. heavy: {vertex, first, end, chunk offset} records.
+    uint4* heavy;
+    uint32_t heavy_cap;
+    uint32_t heavy_min;
 };
+
+__device__ __forceinline__ uint32_t* summary_buf(const BfsArgs& a, uint32_t level) {
+    const uint32_t m = level % 3;
+    return m == 0 ? a.summary0 : (m == 1 ? a.summary1 : a.summary2);
+}
+
+__device__ __forceinline__ void summary_set(const BfsArgs& a, uint32_t* sum, uint32_t word) {
+    const uint32_t sb = word >> a.sum_shift;
+    atomicOr(&sum[sb >> 5], 1u << (sb & 31));
+}
+
+// Neighbours a lane scans alone in the pull phase before the warp takes over.
+constexpr uint32_t kPullLaneScan = 32;
+// Neighbours per piece of a heavy (very long) in-neighbour list.
+constexpr uint32_t kHeavyChunk = 256;
 
 __device__ __forceinline__ uint32_t* frontier_buf(const BfsArgs& a, uint32_t level) {
     const uint32_t m = level % 3;
@@ -63,64 +92,19 @@ __device__ __forceinline__ uint32_t rset_units(const DevGraph& g, uint32_t r) {
     return ALIGNED ? (t + 31) / 32 : t;
 }
 
-__global__ void bfs_init_kernel(BfsArgs a) {
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t nth = gridDim.x * blockDim.x;
-    const uint32_t n = a.g.n, src = a.src;
-    for (uint32_t v = tid; v < n; v += nth) {
-        a.levels[v] = v == src ? 0u : kUnreached;
-        if (a.parents) a.parents[v] = v == src ? src : kUnreached;
-    }
-    const uint32_t sw = src >> 5, sb = 1u << (src & 31);
-    for (uint32_t i = tid; i < a.words; i += nth) {
-        a.visited[i] = i == sw ? sb : 0u;
-        a.frontier0[i] = i == sw ? sb : 0u;
-        a.frontier1[i] = 0u;
-        a.frontier2[i] = 0u;
-    }
-}
-
-// Writes the level-0 state; one thread (after bfs_init_kernel).
-template <bool ALIGNED>
-__global__ void bfs_seed_kernel(BfsArgs a) {
-    RunCounters* c = a.ctr;
-    const uint32_t r = a.src >> 3;
-    const uint32_t units = rset_units<ALIGNED>(a.g, r);
-    uint64_t q = 0;
-    if (units) {
-        a.q_rset[0] = r;
-        a.q_off[0] = 0;
-        q = (1ull << kQShift) | units;
-    }
-    const uint64_t deg = a.g.csr_ptrs[a.src + 1] - a.g.csr_ptrs[a.src];
-    c->queue = q;
-    c->discovered = 1;
-    c->degree = deg;
-    c->grab[0] = c->grab[1] = 0;
-    c->bar_count = 0;
-    c->bar_gen = 0;
-    c->error = 0;
-    c->levels = 0;
-    c->push_levels = 0;
-    c->pull_levels = 0;
-    c->iterations = 0;
-    c->snap_queue[0] = q;
-    c->snap_discovered[0] = 1;
-    c->snap_degree[0] = deg;
-    c->snap_queue[1] = c->snap_discovered[1] = c->snap_degree[1] = 0;
-}
-
-// Per-warp accumulator of enqueue requests, flushed with one atomic.
+// Per-lane buffer of rsets to enqueue, flushed warp-wide with one atomic
+// once some lane holds more than the caller's limit (or at level end).
+constexpr uint32_t kEnqueueCap = 8;
 struct Enqueue {
-    uint32_t rset[4];
+    uint32_t rset[kEnqueueCap];
     uint32_t cnt;
     uint32_t units;
 };
 
 template <bool ALIGNED>
-__device__ __forceinline__ void flush_enqueue(const BfsArgs& a, Enqueue& q) {
+__device__ __forceinline__ void flush_enqueue(const BfsArgs& a, Enqueue& q, int limit = -1) {
     const uint32_t lane = threadIdx.x & 31;
-    if (!__any_sync(0xFFFFFFFFu, q.cnt != 0)) return;
+    if (!__any_sync(0xFFFFFFFFu, (int)q.cnt > limit)) return;
     const uint64_t mine = ((uint64_t)q.cnt << kQShift) | q.units;
     const uint64_t incl = warp_inclusive_scan64(mine);
     uint64_t base = 0;
@@ -144,8 +128,9 @@ __device__ __forceinline__ void flush_enqueue(const BfsArgs& a, Enqueue& q) {
 // single winner, which records level/parent, sets the frontier bit and,
 // when it is the first new vertex of its rset this level, queues the rset.
 template <bool ALIGNED, bool PARENTS>
-__device__ __forceinline__ void discover(const BfsArgs& a, uint32_t* fcur, uint32_t row, uint32_t parent,
-                                         uint32_t level, Enqueue& q, uint32_t& disc, uint64_t& deg) {
+__device__ __forceinline__ void discover(const BfsArgs& a, uint32_t* fcur, uint32_t* fsum, uint32_t row,
+                                         uint32_t parent, uint32_t level, Enqueue& q, uint32_t& disc,
+                                         uint64_t& deg) {
     if (row >= a.g.n) {
         set_error(a.ctr, BLEST_ERR_DEVICE_INDEX);
         return;
@@ -165,8 +150,75 @@ __device__ __forceinline__ void discover(const BfsArgs& a, uint32_t* fcur, uint3
         if (units) {
             q.rset[q.cnt++] = r;
             q.units += units;
+            summary_set(a, fsum, w);
         }
     }
+}
+
+
+// One push step's operands: the tile of this lane (row ids, mask word),
+// the frontier byte of its rset, and the queue owner of the next step.
+struct StepLoad {
+    uint4 rows;
+    uint32_t mask;
+    uint32_t fb;
+    uint32_t r;
+    uint32_t next_owner;
+};
+
+// Resolve the queue entry of each lane's position in the step starting at
+// unit `base` (entries owner..owner+31 can cover it) and issue its loads.
+template <bool ALIGNED>
+__device__ __forceinline__ StepLoad load_step(const BfsArgs& a, const uint32_t* fprev, uint32_t owner, uint32_t E1,
+                                              uint32_t U1, uint32_t base, RunCounters* c) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t ei = owner + lane;
+    const bool in = ei < E1;
+    const uint32_t eoff = in ? __ldcg(&a.q_off[ei]) : 0xFFFFFFFFu;
+    const uint32_t ers = in ? __ldcg(&a.q_rset[ei]) : 0u;
+    uint32_t pos, my;
+    if (ALIGNED) {
+        pos = base;
+        my = __popc(__ballot_sync(0xFFFFFFFFu, eoff <= pos)) - 1;
+    } else {
+        pos = base + lane;
+        uint32_t lo = 0;
+#pragma unroll
+        for (uint32_t st = 16; st > 0; st >>= 1) {
+            const uint32_t cand = lo + st;
+            const uint32_t b = __shfl_sync(0xFFFFFFFFu, eoff, cand & 31);
+            if (cand < 32 && b <= pos) lo = cand;
+        }
+        my = lo;
+    }
+    StepLoad L;
+    L.r = __shfl_sync(0xFFFFFFFFu, ers, my);
+    const uint32_t off = __shfl_sync(0xFFFFFFFFu, eoff, my);
+    L.next_owner = owner + __shfl_sync(0xFFFFFFFFu, my, 31);
+    const uint32_t t0 = __ldg(&a.g.rset_tile[L.r]);
+    const uint32_t t1 = __ldg(&a.g.rset_tile[L.r + 1]);
+    uint32_t tile;
+    bool valid;
+    if (ALIGNED) {
+        tile = t0 + (pos - off) * 32 + lane;
+        valid = tile < t1;
+    } else {
+        tile = t0 + (pos - off);
+        valid = pos < U1;
+    }
+    if (valid && (pos < off || tile >= t1)) {
+        // queue offsets inconsistent with the rset's tiles: never read past it
+        set_error(c, BLEST_ERR_DEVICE_INDEX);
+        valid = false;
+    }
+    L.fb = (__ldcg(&fprev[L.r >> 2]) >> (8 * (L.r & 3))) & 0xFFu;
+    L.rows = make_uint4(0, 0, 0, 0);
+    L.mask = 0;
+    if (valid) {
+        L.rows = ld_stream(&a.g.row4[tile]);
+        L.mask = ld_stream(&a.g.masks[tile]);
+    }
+    return L;
 }
 
 // mma.sync m8n8k128 b1 AND+POPC: d[i] = popc(A_row & B_col) per the PTX
@@ -214,8 +266,51 @@ __device__ __forceinline__ uint32_t find_owner(const uint32_t* q_off, uint32_t l
     return lo + __popc(__ballot_sync(0xFFFFFFFFu, ok)) - 1;
 }
 
+// Level-0 state, written by the persistent kernel itself before its first
+// barrier (saves the separate init and seed launches): levels/parents
+// reset, bitmaps and summaries cleared with the source's bits set, and the
+// source's rset queued. The run counters were zeroed by the launcher.
+template <bool ALIGNED>
+__device__ __forceinline__ void bfs_prologue(const BfsArgs& a, uint32_t tid, uint32_t nth) {
+    const uint32_t n = a.g.n, src = a.src;
+    for (uint32_t v = tid; v < n; v += nth) {
+        a.levels[v] = v == src ? 0u : kUnreached;
+        if (a.parents) a.parents[v] = v == src ? src : kUnreached;
+    }
+    const uint32_t sw = src >> 5, sb = 1u << (src & 31);
+    for (uint32_t i = tid; i < a.words; i += nth) {
+        a.visited[i] = i == sw ? sb : 0u;
+        a.frontier0[i] = i == sw ? sb : 0u;
+        a.frontier1[i] = 0u;
+        a.frontier2[i] = 0u;
+    }
+    const uint32_t units = rset_units<ALIGNED>(a.g, src >> 3);
+    const uint32_t ssb = sw >> a.sum_shift;
+    for (uint32_t i = tid; i < a.sum_words; i += nth) {
+        a.summary0[i] = (units && i == (ssb >> 5)) ? (1u << (ssb & 31)) : 0u;
+        a.summary1[i] = 0u;
+        a.summary2[i] = 0u;
+    }
+    if (tid == 0) {
+        RunCounters* c = a.ctr;
+        uint64_t q = 0;
+        if (units) {
+            a.q_rset[0] = src >> 3;
+            a.q_off[0] = 0;
+            q = (1ull << kQShift) | units;
+        }
+        const uint64_t deg = a.g.csr_ptrs[src + 1] - a.g.csr_ptrs[src];
+        c->queue = q;
+        c->discovered = 1;
+        c->degree = deg;
+        c->snap_queue[0] = q;
+        c->snap_discovered[0] = 1;
+        c->snap_degree[0] = deg;
+    }
+}
+
 template <bool ALIGNED, bool MMA, bool PARENTS>
-__global__ void __launch_bounds__(512) bfs_persistent_kernel(BfsArgs a) {
+__global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(BfsArgs a) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t nth = gridDim.x * blockDim.x;
@@ -223,6 +318,9 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(BfsArgs a) {
     const uint32_t nwarps = nth >> 5;
     const DevGraph& g = a.g;
     RunCounters* c = a.ctr;
+
+    bfs_prologue<ALIGNED>(a, tid, nth);
+    if (!grid_barrier(c, 1)) return;
 
     // Cumulative counters at the end of levels L-3 and L-2.
     uint32_t E3 = 0, E2 = 0, U2 = 0;
@@ -236,7 +334,17 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(BfsArgs a) {
         const uint64_t D1 = c->snap_discovered[par], G1 = c->snap_degree[par];
         const uint64_t nf = D1 - D2;  // discovered at level L-1
         if (nf == 0) {
-            if (tid == 0) c->levels = level - 1;  // max level + 1
+            if (tid == 0) {
+                c->levels = level - 1;  // max level + 1
+                if (a.trace && level <= BLEST_TRACE_CAPACITY) {
+                    blest_level_trace& t = a.trace[level - 1];
+                    t.start_ns = global_ns();
+                    t.level = level;
+                    t.direction = 0;
+                    t.frontier = 0;
+                    t.work_units = 0;
+                }
+            }
             break;
         }
         if (level > g.n + 1) {
@@ -244,13 +352,33 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(BfsArgs a) {
             break;
         }
         if (a.direction == BLEST_DIR_AUTO) {
+            // Beamer's switch in edge/vertex units: to pull when the new
+            // frontier's edges m_f exceed the unvisited edges m_u / alpha,
+            // back to push when the new frontier has fewer than n / beta
+            // vertices.
             const double mf = (double)(G1 - G2), mu = (double)(g.degree_total - G1);
             if (dir == BLEST_DIR_PUSH && mf * a.alpha > mu) dir = BLEST_DIR_PULL;
             else if (dir == BLEST_DIR_PULL && (double)nf * a.beta < (double)g.n) dir = BLEST_DIR_PUSH;
         }
+        if (a.trace && tid == 0 && level <= BLEST_TRACE_CAPACITY) {
+            blest_level_trace& t = a.trace[level - 1];
+            t.start_ns = global_ns();
+            t.level = level;
+            t.direction = (uint32_t)dir;
+            t.frontier = nf;
+            t.work_units = (uint64_t)(U1 - U2);
+            // longest warp-finished scan of the previous level; its slot is
+            // then free for the next level
+            if (level >= 2) a.trace[level - 2].longest_scan = ld_relaxed64(&c->aux[6 + ((level - 1) & 1)]);
+            c->aux[6 + ((level - 1) & 1)] = 0;
+        }
+        // heavy-list counter of the next level (its slot was last used at level-1)
+        if (tid == 0) c->aux[2 + ((level + 1) & 1)] = 0;
         uint32_t* fprev = frontier_buf(a, level - 1);
         uint32_t* fcur = frontier_buf(a, level);
         uint8_t* fclr = reinterpret_cast<uint8_t*>(frontier_buf(a, level + 1));
+        uint32_t* fsum = summary_buf(a, level);
+        uint32_t* sclr = summary_buf(a, level + 1);
 
         Enqueue q;
         q.cnt = 0;
@@ -268,125 +396,222 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(BfsArgs a) {
             if (s < send) {
                 uint32_t owner = find_owner(a.q_off, E2, E1, U2 + s * per);
                 for (; s < send; ++s) {
-                    const uint32_t base = U2 + s * per;
-                    // Entry bounds for the (up to 32) entries this step can touch.
-                    const uint32_t ei = owner + lane;
-                    const bool in = ei < E1;
-                    const uint32_t eoff = in ? __ldcg(&a.q_off[ei]) : 0xFFFFFFFFu;
-                    const uint32_t ers = in ? __ldcg(&a.q_rset[ei]) : 0u;
-                    uint32_t pos, my;
-                    if (ALIGNED) {
-                        pos = base;
-                        my = 0;
-                        // warp-uniform owner of this chunk
-                        my = __popc(__ballot_sync(0xFFFFFFFFu, eoff <= pos)) - 1;
-                    } else {
-                        pos = base + lane;
-                        uint32_t lo = 0;
-#pragma unroll
-                        for (uint32_t st = 16; st > 0; st >>= 1) {
-                            const uint32_t cand = lo + st;
-                            const uint32_t b = __shfl_sync(0xFFFFFFFFu, eoff, cand & 31);
-                            if (cand < 32 && b <= pos) lo = cand;
-                        }
-                        my = lo;
-                    }
-                    const uint32_t r = __shfl_sync(0xFFFFFFFFu, ers, my);
-                    const uint32_t off = __shfl_sync(0xFFFFFFFFu, eoff, my);
-                    owner += __shfl_sync(0xFFFFFFFFu, my, 31);
-                    const uint32_t t0 = __ldg(&g.rset_tile[r]);
-                    const uint32_t t1 = __ldg(&g.rset_tile[r + 1]);
-                    uint32_t tile;
-                    bool valid;
-                    if (ALIGNED) {
-                        tile = t0 + (pos - off) * 32 + lane;
-                        valid = tile < t1;
-                    } else {
-                        tile = t0 + (pos - off);
-                        valid = pos < U1;
-                    }
-                    if (valid && (pos < off || tile >= t1)) {
-                        // queue offsets inconsistent with the rset's tiles: never read past it
-                        set_error(c, BLEST_ERR_DEVICE_INDEX);
-                        valid = false;
-                    }
-                    const uint32_t fb = (__ldcg(&fprev[r >> 2]) >> (8 * (r & 3))) & 0xFFu;
-                    uint4 rows = make_uint4(0, 0, 0, 0);
-                    uint32_t mask = 0;
-                    if (valid) {
-                        rows = ld_stream(&g.row4[tile]);
-                        mask = ld_stream(&g.masks[tile]);
-                    }
+                    const StepLoad cur = load_step<ALIGNED>(a, fprev, owner, E1, U1, U2 + s * per, c);
+                    owner = cur.next_owner;
                     uint32_t hits;
                     if (MMA) {
-                        hits = hits_mma(mask, fb);
+                        hits = hits_mma(cur.mask, cur.fb);
                     } else {
                         hits = 0;
 #pragma unroll
-                        for (uint32_t kk = 0; kk < 4; ++kk) hits |= (((mask >> (8 * kk)) & fb & 0xFFu) ? 1u : 0u) << kk;
+                        for (uint32_t kk = 0; kk < 4; ++kk)
+                            hits |= (((cur.mask >> (8 * kk)) & cur.fb & 0xFFu) ? 1u : 0u) << kk;
                     }
                     if (hits) {
-                        const uint32_t rowk[4] = {rows.x, rows.y, rows.z, rows.w};
+                        const uint32_t rowk[4] = {cur.rows.x, cur.rows.y, cur.rows.z, cur.rows.w};
 #pragma unroll
                         for (uint32_t kk = 0; kk < 4; ++kk) {
                             if (hits & (1u << kk)) {
-                                const uint32_t hb = (mask >> (8 * kk)) & fb & 0xFFu;
-                                const uint32_t parent = r * 8 + (__ffs(hb) - 1);
-                                discover<ALIGNED, PARENTS>(a, fcur, rowk[kk], parent, level, q, disc, deg);
+                                const uint32_t hb = (cur.mask >> (8 * kk)) & cur.fb & 0xFFu;
+                                discover<ALIGNED, PARENTS>(a, fcur, fsum, rowk[kk], cur.r * 8 + (__ffs(hb) - 1),
+                                                           level, q, disc, deg);
                             }
                         }
                     }
-                    flush_enqueue<ALIGNED>(a, q);
+                    flush_enqueue<ALIGNED>(a, q, kEnqueueCap - 4);
                 }
             }
         } else {
-            // Bottom-up: each warp owns whole 32-vertex words.
+            // Bottom-up: each warp owns whole 32-vertex words. Each lane scans
+            // its unvisited vertex's in-neighbours four at a time
+            // (independent loads) for at most kPullLaneScan neighbours; the
+            // warp then finishes the longer lists together, one vertex at a
+            // time, 32 neighbours per coalesced step, stopping at the first
+            // frontier neighbour. A neighbour's frontier word is read from L2
+            // only when the level's summary (staged in shared memory) says
+            // it is non-empty; vertices without in-neighbours are skipped.
+            extern __shared__ uint32_t s_sum[];
+            const uint32_t* sprev = summary_buf(a, level - 1);
+            for (uint32_t i = threadIdx.x; i < a.sum_words; i += blockDim.x) s_sum[i] = __ldcg(&sprev[i]);
+            __syncthreads();
+            auto in_frontier = [&](uint32_t v) -> bool {
+                const uint32_t sb = (v >> 5) >> a.sum_shift;
+                if (!((s_sum[sb >> 5] >> (sb & 31)) & 1u)) return false;
+                return (__ldcg(&fprev[v >> 5]) >> (v & 31)) & 1u;
+            };
             const uint32_t W = (g.n + 31) / 32;
             const uint32_t tailMask = (g.n & 31) ? ((1u << (g.n & 31)) - 1) : 0xFFFFFFFFu;
-            for (uint32_t i = warp; i < W; i += nwarps) {
-                const uint32_t vis = __ldcg(&a.visited[i]);
-                const uint32_t unv = ~vis & (i == W - 1 ? tailMask : 0xFFFFFFFFu);
+            uint32_t longest = 0;
+            // The next word's visited/has-in words and row bounds are loaded
+            // while the current word is scanned (software pipeline).
+            uint32_t nvis = 0, nhin = 0xFFFFFFFFu, npb = 0, npe = 0;
+            auto prefetch = [&](uint32_t w) {
+                if (w < W) {
+                    nvis = __ldcg(&a.visited[w]);
+                    nhin = g.has_in ? __ldg(&g.has_in[w]) : 0xFFFFFFFFu;
+                    const uint32_t v = w * 32 + lane;
+                    npb = v < g.n ? __ldg(&g.csr_ptrs[v]) : 0u;
+                    npe = v < g.n ? __ldg(&g.csr_ptrs[v + 1]) : 0u;
+                }
+            };
+            prefetch(warp);
+            for (uint32_t wi = warp; wi < W; wi += nwarps) {
+                const uint32_t vis = nvis, hin = nhin, rb = npb, re = npe;
+                prefetch(wi + nwarps);
+                uint32_t unv = ~vis & (wi == W - 1 ? tailMask : 0xFFFFFFFFu) & hin;
                 if (unv == 0) continue;
                 bool found = false;
                 uint32_t parent = kUnreached;
-                const uint32_t u = i * 32 + lane;
+                const uint32_t u = wi * 32 + lane;
+                uint32_t pb = 0, pe = 0, p = 0;
                 if ((unv >> lane) & 1u) {
-                    const uint32_t pb = __ldg(&g.csr_ptrs[u]), pe = __ldg(&g.csr_ptrs[u + 1]);
-                    for (uint32_t p = pb; p < pe; ++p) {
-                        const uint32_t v = __ldg(&g.csr_ids[p]);
-                        if ((__ldcg(&fprev[v >> 5]) >> (v & 31)) & 1u) {
-                            found = true;
-                            parent = v;
+                    pb = rb;
+                    pe = re;
+                    p = pb;
+                    const uint32_t cap = pb + min(pe - pb, kPullLaneScan);
+                    for (; p < cap && !found; p += 4) {
+                        uint32_t v[4];
+                        bool f[4];
+#pragma unroll
+                        for (uint32_t j = 0; j < 4; ++j) v[j] = p + j < pe ? __ldg(&g.csr_ids[p + j]) : kUnreached;
+#pragma unroll
+                        for (uint32_t j = 0; j < 4; ++j) f[j] = v[j] != kUnreached && in_frontier(v[j]);
+#pragma unroll
+                        for (uint32_t j = 0; j < 4; ++j) {
+                            if (!found && f[j]) {
+                                found = true;
+                                parent = v[j];
+                            }
+                        }
+                    }
+                }
+                // Very long lists go to the heavy queue (all warps split them
+                // after the mid-level barrier).
+                {
+                    const bool heavy = !found && p < pe && pe - p > a.heavy_min;
+                    if (heavy) {
+                        const uint32_t chunks = (pe - p + kHeavyChunk - 1) / kHeavyChunk;
+                        const uint64_t slot = atomicAdd(&c->aux[2 + (level & 1)],
+                                                        (unsigned long long)((1ull << kQShift) | chunks));
+                        const uint32_t idx = (uint32_t)(slot >> kQShift);
+                        if (idx < a.heavy_cap) {
+                            a.heavy[idx] = make_uint4(u, p, pe, (uint32_t)(slot & kQUnitMask));
+                            p = pe;  // handed over
+                        } else {
+                            set_error(c, BLEST_ERR_DEVICE_INDEX);  // capacity is sized so this cannot happen
+                        }
+                    }
+                }
+                // Long lists: the whole warp scans them, one vertex at a time.
+                uint32_t rest = __ballot_sync(0xFFFFFFFFu, !found && p < pe);
+                while (rest) {
+                    const uint32_t ln = __ffs(rest) - 1;
+                    rest &= rest - 1;
+                    const uint32_t q0 = __shfl_sync(0xFFFFFFFFu, p, ln);
+                    const uint32_t q1 = __shfl_sync(0xFFFFFFFFu, pe, ln);
+                    longest = max(longest, q1 - q0);
+                    uint32_t hitv = kUnreached;
+                    for (uint32_t base = q0; base < q1; base += 32) {
+                        const uint32_t idx = base + lane;
+                        const uint32_t v = idx < q1 ? __ldg(&g.csr_ids[idx]) : kUnreached;
+                        const bool f = v != kUnreached && in_frontier(v);
+                        const uint32_t hb = __ballot_sync(0xFFFFFFFFu, f);
+                        if (hb) {
+                            hitv = __shfl_sync(0xFFFFFFFFu, v, __ffs(hb) - 1);
                             break;
                         }
+                    }
+                    if (lane == ln && hitv != kUnreached) {
+                        found = true;
+                        parent = hitv;
                     }
                 }
                 const uint32_t nb = __ballot_sync(0xFFFFFFFFu, found);
                 if (nb == 0) continue;
                 if (lane == 0) {
-                    a.visited[i] = vis | nb;
-                    fcur[i] = nb;
+                    a.visited[wi] = vis | nb;
+                    fcur[wi] = nb;
                 }
                 if (found) {
                     a.levels[u] = level;
                     if (PARENTS) a.parents[u] = parent;
                     ++disc;
-                    deg += __ldg(&g.csr_ptrs[u + 1]) - __ldg(&g.csr_ptrs[u]);
+                    deg += pe - pb;
                 }
+                bool queued = false;
                 if (lane < 4 && ((nb >> (8 * lane)) & 0xFFu)) {
-                    const uint32_t r = i * 4 + lane;
+                    const uint32_t r = wi * 4 + lane;
                     const uint32_t units = rset_units<ALIGNED>(g, r);
                     if (units) {
                         q.rset[q.cnt++] = r;
                         q.units += units;
+                        queued = true;
                     }
                 }
-                flush_enqueue<ALIGNED>(a, q);
+                if (__ballot_sync(0xFFFFFFFFu, queued) && lane == 0) summary_set(a, fsum, wi);
+                flush_enqueue<ALIGNED>(a, q, kEnqueueCap - 1);
+            }
+            if (a.trace && lane == 0 && longest) atomicMax(&c->aux[6 + (level & 1)], (unsigned long long)longest);
+            flush_enqueue<ALIGNED>(a, q);
+            // Heavy lists: every warp takes an equal share of the pieces.
+            if (!grid_barrier(c, level & 1)) return;
+            const uint64_t hq = ld_relaxed64(&c->aux[2 + (level & 1)]);
+            const uint32_t hitems = min((uint32_t)(hq >> kQShift), a.heavy_cap);
+            const uint32_t hchunks = (uint32_t)(hq & kQUnitMask);
+            if (hitems) {
+                const uint32_t hk = (hchunks + nwarps - 1) / nwarps;
+                for (uint32_t ch = warp * hk; ch < min(hchunks, warp * hk + hk); ++ch) {
+                    // owner: largest item with chunk offset <= ch
+                    uint32_t lo = 0, hi = hitems;
+                    while (hi - lo > 1) {
+                        const uint32_t mid = (lo + hi) / 2;
+                        if (__ldcg(&a.heavy[mid].w) <= ch) lo = mid;
+                        else hi = mid;
+                    }
+                    const uint4 it = __ldcg(&a.heavy[lo]);
+                    const uint32_t hu = it.x, w = hu >> 5, b = 1u << (hu & 31);
+                    const uint32_t q0 = it.y + (ch - it.w) * kHeavyChunk;
+                    const uint32_t q1 = min(it.z, q0 + kHeavyChunk);
+                    uint32_t hitv = kUnreached;
+                    for (uint32_t base = q0; base < q1 && hitv == kUnreached; base += 32) {
+                        if (__ldcg(&a.visited[w]) & b) break;  // another piece found it
+                        const uint32_t idx = base + lane;
+                        const uint32_t v = idx < q1 ? __ldg(&g.csr_ids[idx]) : kUnreached;
+                        const bool f = v != kUnreached && in_frontier(v);
+                        const uint32_t hb = __ballot_sync(0xFFFFFFFFu, f);
+                        if (hb) hitv = __shfl_sync(0xFFFFFFFFu, v, __ffs(hb) - 1);
+                    }
+                    if (hitv != kUnreached && lane == 0) {
+                        const uint32_t old = atomicOr(&a.visited[w], b);
+                        if (!(old & b)) {
+                            a.levels[hu] = level;
+                            if (PARENTS) a.parents[hu] = hitv;
+                            ++disc;
+                            deg += __ldg(&g.csr_ptrs[hu + 1]) - __ldg(&g.csr_ptrs[hu]);
+                            const uint32_t oldF = atomicOr(&fcur[w], b);
+                            if (((oldF >> (hu & 24)) & 0xFFu) == 0) {
+                                const uint32_t r = hu >> 3;
+                                const uint32_t units = rset_units<ALIGNED>(g, r);
+                                if (units) {
+                                    q.rset[q.cnt++] = r;
+                                    q.units += units;
+                                    summary_set(a, fsum, w);
+                                }
+                            }
+                        }
+                    }
+                    flush_enqueue<ALIGNED>(a, q, kEnqueueCap - 1);
+                }
             }
         }
 
+        flush_enqueue<ALIGNED>(a, q);  // whatever is still buffered
         // Clear the frontier bytes written two levels back (queue of L-2).
-        for (uint32_t e = E3 + tid; e < E2; e += nth) fclr[__ldcg(&a.q_rset[e])] = 0;
+        for (uint32_t e = E3 + tid; e < E2; e += nth) {
+            const uint32_t r = __ldcg(&a.q_rset[e]);
+            fclr[r] = 0;
+            sclr[((r >> 2) >> a.sum_shift) >> 5] = 0u;
+        }
 
         const uint64_t wd = warp_sum64(disc), wg = warp_sum64(deg);
         if (lane == 0 && wd) {
@@ -414,17 +639,16 @@ template <bool ALIGNED, bool MMA, bool PARENTS>
 void launch_variant(const blest_graph* g, const dev::BfsArgs& args, int blocks_per_sm, int threads,
                     cudaStream_t s) {
     auto kern = dev::bfs_persistent_kernel<ALIGNED, MMA, PARENTS>;
+    const size_t smem = 4ull * args.sum_words;
+    BLEST_CUDA(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int maxBlocks = 0;
-    BLEST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxBlocks, kern, threads, 0));
+    BLEST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxBlocks, kern, threads, smem));
     if (maxBlocks < 1) throw Error(BLEST_ERR_CUDA, "BFS kernel cannot be resident with this block size");
     const int bps = blocks_per_sm > 0 ? std::min(blocks_per_sm, maxBlocks) : maxBlocks;
     const int grid = bps * g->sm_count;
-    dev::bfs_init_kernel<<<g->sm_count * 4, 512, 0, s>>>(args);
-    BLEST_CUDA(cudaGetLastError());
-    dev::bfs_seed_kernel<ALIGNED><<<1, 1, 0, s>>>(args);
-    BLEST_CUDA(cudaGetLastError());
+    BLEST_CUDA(cudaMemsetAsync(args.ctr, 0, sizeof(dev::RunCounters), s));
     void* kargs[] = {(void*)&args};
-    BLEST_CUDA(cudaLaunchCooperativeKernel((void*)kern, grid, threads, kargs, 0, s));
+    BLEST_CUDA(cudaLaunchCooperativeKernel((void*)kern, grid, threads, kargs, smem, s));
 }
 
 }  // namespace
@@ -447,6 +671,15 @@ void launch_bfs(const blest_graph* g, Workspace& w, uint32_t src, uint32_t* leve
     a.direction = p.direction;
     a.alpha = p.alpha > 0 ? (float)p.alpha : 14.0f;
     a.beta = p.beta > 0 ? (float)p.beta : 24.0f;
+    a.trace = p.trace ? w.trace : nullptr;
+    a.summary0 = w.summary[0];
+    a.summary1 = w.summary[1];
+    a.summary2 = w.summary[2];
+    a.sum_shift = w.sum_shift;
+    a.sum_words = w.sum_words;
+    a.heavy = w.heavy;
+    a.heavy_cap = w.heavy_cap;
+    a.heavy_min = heavy_threshold(g->d.nnz, w.heavy_cap);
     const int threads = p.threads_per_block > 0 ? p.threads_per_block : 512;
     if (threads % 32 || threads > 512) throw Error(BLEST_ERR_INVALID_ARG, "threads_per_block must be a multiple of 32, <= 512");
     const bool mma = p.slice_test == BLEST_TEST_B1_MMA;
@@ -486,7 +719,11 @@ constexpr size_t kNaFrontier = kNaVisited + 4ull * kNoAllocWords;     // 3 bitma
 constexpr size_t kNaRsetTile = kNaFrontier + 3 * 4ull * kNoAllocWords;
 constexpr size_t kNaQRset = kNaRsetTile + 4ull * (kNoAllocRsets + 64);
 constexpr size_t kNaQOff = kNaQRset + 4ull * kNoAllocQueue;
-constexpr size_t kNaCounters = (kNaQOff + 4ull * kNoAllocQueue + 255) & ~size_t(255);
+constexpr uint32_t kNoAllocSumWords = (kNoAllocWords + 31) / 32;       // summary words (shift 0)
+constexpr size_t kNaSummary = kNaQOff + 4ull * kNoAllocQueue;         // 3 summaries
+constexpr uint32_t kNoAllocHeavy = 4096;                              // heavy-list records
+constexpr size_t kNaHeavy = (kNaSummary + 3 * 4ull * kNoAllocSumWords + 15) & ~size_t(15);
+constexpr size_t kNaCounters = (kNaHeavy + 16ull * kNoAllocHeavy + 255) & ~size_t(255);
 constexpr size_t kNoAllocBytes = kNaCounters + ((sizeof(dev::RunCounters) + 255) & ~size_t(255));
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
@@ -503,15 +740,14 @@ __global__ void noalloc_rset_tile_kernel(const uint64_t* ssp, const uint32_t* re
 template <bool PARENTS>
 void noalloc_launch(const dev::BfsArgs& a, int sms, cudaStream_t s) {
     auto kern = dev::bfs_persistent_kernel<false, false, PARENTS>;
+    const size_t smem = 4ull * a.sum_words;
+    BLEST_CUDA(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int maxBlocks = 0;
-    BLEST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxBlocks, kern, 512, 0));
+    BLEST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxBlocks, kern, 512, smem));
     if (maxBlocks < 1) throw Error(BLEST_ERR_CUDA, "BFS kernel cannot be resident");
-    dev::bfs_init_kernel<<<sms * 4, 512, 0, s>>>(a);
-    BLEST_CUDA(cudaGetLastError());
-    dev::bfs_seed_kernel<false><<<1, 1, 0, s>>>(a);
-    BLEST_CUDA(cudaGetLastError());
+    BLEST_CUDA(cudaMemsetAsync(a.ctr, 0, sizeof(dev::RunCounters), s));
     void* kargs[] = {(void*)&a};
-    BLEST_CUDA(cudaLaunchCooperativeKernel((void*)kern, maxBlocks * sms, 512, kargs, 0, s));
+    BLEST_CUDA(cudaLaunchCooperativeKernel((void*)kern, maxBlocks * sms, 512, kargs, smem, s));
 }
 
 }  // namespace
@@ -572,6 +808,14 @@ extern "C" int blest_bfs_noalloc(const blest_device_graph_view* g, uint32_t sour
         a.q_off = (uint32_t*)(base + kNaQOff);
         a.ctr = (dev::RunCounters*)(base + kNaCounters);
         a.words = ((g->n + 31) / 32 + 3) & ~3u;
+        summary_geometry(a.words, a.sum_shift, a.sum_words);
+        if (a.sum_words > kNoAllocSumWords) throw Error(BLEST_ERR_UNSUPPORTED, "summary does not fit the scratch");
+        a.summary0 = (uint32_t*)(base + kNaSummary);
+        a.summary1 = a.summary0 + kNoAllocSumWords;
+        a.summary2 = a.summary1 + kNoAllocSumWords;
+        a.heavy = (uint4*)(base + kNaHeavy);
+        a.heavy_cap = kNoAllocHeavy;
+        a.heavy_min = heavy_threshold(g->nnz, kNoAllocHeavy);
         a.src = source;
         a.direction = BLEST_DIR_AUTO;
         a.alpha = 14.0f;

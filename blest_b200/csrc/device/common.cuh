@@ -38,6 +38,7 @@ struct DevGraph {
     const uint32_t* rset_tile;  // R + 1
     const uint32_t* csr_ptrs;   // n + 1 (in-neighbours)
     const uint32_t* csr_ids;    // nnz
+    const uint32_t* has_in;     // ceil(n/32) words: bit v = v has an in-neighbour (may be null)
 };
 
 // Counters of one BFS/CC run (zeroed by the init kernel).

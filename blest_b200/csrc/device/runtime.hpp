@@ -32,6 +32,12 @@ struct Workspace {
     uint32_t* parents = nullptr;
     uint32_t* labels_old = nullptr;  // CC
     dev::RunCounters* host_counters = nullptr;  // pinned mirror
+    blest_level_trace* trace = nullptr;         // device, BLEST_TRACE_CAPACITY records
+    uint32_t* summary[3] = {nullptr, nullptr, nullptr};  // frontier summaries
+    uint32_t sum_shift = 0;                     // frontier words per summary bit = 2^sum_shift
+    uint32_t sum_words = 0;                     // 32-bit words per summary
+    uint4* heavy = nullptr;                     // pull: very long in-neighbour lists
+    uint32_t heavy_cap = 0;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     uint64_t bytes = 0;
 };
@@ -64,6 +70,15 @@ struct blest_workspace {
 namespace blest {
 
 void workspace_alloc(const blest_graph* g, Workspace& w);
+// Summary geometry: the smallest shift whose summary fits kSummaryMaxBytes.
+constexpr uint32_t kSummaryMaxBytes = 64 * 1024;
+void summary_geometry(uint32_t words, uint32_t& shift, uint32_t& sum_words);
+// Remaining-list length above which a pull vertex goes to the heavy queue:
+// at least 1024, and large enough that nnz / threshold records fit `cap`.
+inline uint32_t heavy_threshold(uint32_t nnz, uint32_t cap) {
+    const uint64_t t = ((uint64_t)nnz + cap - 1) / cap;
+    return (uint32_t)(t > 1024 ? t : 1024);
+}
 void workspace_free(Workspace& w);
 
 // Kernel launchers (bfs.cu, cc.cu). Outputs are device pointers.

@@ -283,10 +283,10 @@ def init(device: int = 0) -> None:
 
 
 def bfs_params(direction: str = "auto", slice_test: str = "cuda_core", alpha: float = 0.0, beta: float = 0.0,
-               blocks_per_sm: int = 0, threads_per_block: int = 0) -> L.BfsParams:
+               blocks_per_sm: int = 0, threads_per_block: int = 0, trace: bool = False) -> L.BfsParams:
     d = {"auto": L.DIR_AUTO, "push": L.DIR_PUSH, "pull": L.DIR_PULL}[direction]
     t = {"cuda_core": L.TEST_CUDA_CORE, "mma": L.TEST_B1_MMA}[slice_test]
-    return L.BfsParams(d, t, alpha, beta, blocks_per_sm, threads_per_block)
+    return L.BfsParams(d, t, alpha, beta, blocks_per_sm, threads_per_block, int(trace))
 
 
 class Graph:
@@ -310,6 +310,21 @@ class Graph:
             self._h = None
 
     __del__ = close
+
+    def trace(self) -> list[dict]:
+        """Per-level records of the last BFS run with bfs_params(trace=True)."""
+        ws = C.c_void_p()
+        L.call("blest_graph_default_workspace", self._h, C.byref(ws))
+        recs = (L.LevelTrace * 4096)()
+        cnt = L.u32()
+        L.call("blest_workspace_trace", ws, recs, 4096, C.byref(cnt))
+        out = []
+        for i in range(cnt.value):
+            r = recs[i]
+            out.append({"level": r.level, "dir": {1: "push", 2: "pull"}.get(r.direction, "end"),
+                        "start_ns": r.start_ns, "frontier": r.frontier, "work_units": r.work_units,
+                        "longest_scan": r.longest_scan})
+        return out
 
     def info(self) -> L.GraphInfo:
         i = L.GraphInfo()

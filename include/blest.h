@@ -233,7 +233,21 @@ typedef struct blest_bfs_params {
     double beta;              /* pull -> push when n_f * beta < n   (0 -> 24) */
     int blocks_per_sm;        /* 0 = occupancy maximum */
     int threads_per_block;    /* 0 = 512 */
+    int trace;                /* != 0: record per-level timestamps in the workspace
+                                 (the reference's commented-out %globaltimer level
+                                 profile, BFS/BVSSBFSKernel.cuh:55-58, 277-282) */
 } blest_bfs_params;
+
+/* One record per BFS level (after a traced run). */
+typedef struct blest_level_trace {
+    uint64_t start_ns;        /* %globaltimer at the start of the level */
+    uint32_t level;
+    uint32_t direction;       /* BLEST_DIR_PUSH or BLEST_DIR_PULL; 0 for the end record */
+    uint64_t frontier;        /* vertices discovered at the previous level */
+    uint64_t work_units;      /* tiles (32-tile chunks with the MMA test) of the queued rsets */
+    uint64_t longest_scan;    /* pull: longest in-neighbour list finished by a whole warp */
+} blest_level_trace;
+#define BLEST_TRACE_CAPACITY 4096
 
 /* Mirrors BFSResult (BFS/BFSKernel.cuh:21-28) plus timing detail. */
 typedef struct blest_bfs_stats {
@@ -257,6 +271,10 @@ int blest_bfs(blest_graph* g, uint32_t source, uint32_t* levels_out, uint32_t* p
 int blest_bfs_ws(blest_workspace* ws, uint32_t source, uint32_t* levels_out, uint32_t* parents_out, int out_mem,
                  const blest_bfs_params* params, void* stream, int async, blest_bfs_stats* stats);
 int blest_workspace_sync(blest_workspace* ws, blest_bfs_stats* stats);
+/* Level records of the last traced BFS on `ws` (at most `max`). */
+int blest_workspace_trace(blest_workspace* ws, blest_level_trace* out, uint32_t max, uint32_t* count);
+/* The default workspace of a graph (owned by the graph). */
+int blest_graph_default_workspace(blest_graph* g, blest_workspace** out);
 
 /* ---- allocation-free single-source BFS ------------------------------------
  * This entry point has no counterpart in the reference.
