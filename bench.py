@@ -45,6 +45,9 @@ WORKLOADS = {
                  "2D 4096x4096 grid, 5% edges deleted, 0.1% shortcuts, RCM, 32 seeded sources"),
     "er25": ("bfs", ("er", 25, 32), "rcm", 0, 32, "Erdos-Renyi 2^25 vertices avg degree 32, RCM, 32 sources"),
     "cc_rmat24": ("cc", ("rmat", 24, 16), "jaccard", 65536, 0, "connected components, RMAT scale 24"),
+    "mbfs_rmat22": ("mbfs", ("rmat", 22, 16), "jaccard", 65536, 1024,
+                    "multi-source BFS, RMAT scale 22 ef 16, Jaccard window 65536, 1024 seeded sources "
+                    "in bit-packed groups of 128"),
 }
 
 SEED = 1
@@ -187,6 +190,116 @@ def profiled_traffic(workload: str):
 
 
 # ----------------------------------------------------------------- arms
+def run_mbfs(args, rank, world):
+    """Multi-source BFS GTEPS (sum over sources of reached edges / batch
+    time), next to the same sources run one BFS launch each."""
+    import torch
+    import torch.distributed as dist
+    import blest_b200
+    from blest_b200 import Graph, Workspace
+    from blest_b200 import _lib as L
+    import ctypes as C
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    blest_b200.init(dev)
+    kind, gen, order, window, nsrc, desc = WORKLOADS[args.workload]
+    csc, bvss, csr, sources = prepare(args.workload, Path(args.cache), rank, world)
+    g = Graph(bvss, csr)
+    n = csc.n
+    k = len(sources)
+    deg = torch.from_numpy(np.diff(csr.col_ptrs.astype(np.int64))).cuda()
+    out = torch.empty((k, n), dtype=torch.int32, device="cuda")
+    src = np.ascontiguousarray(sources, dtype=np.uint32)
+    p = L.MbfsParams(args.group_width, 0, 0)
+    st = L.MbfsStats()
+    barrier = (lambda: dist.barrier()) if world > 1 else (lambda: None)
+
+    def mbfs_once():
+        L.call("blest_mbfs", g._h, src.ctypes.data_as(L.P(L.u32)), k, out.data_ptr(), L.MEM_DEVICE,
+               C.byref(p), C.byref(st))
+
+    mbfs_once()
+    reached = (out != -1)
+    mr = int(((reached.to(torch.int64) * deg).sum(1) // 2).sum().item())
+    del reached
+    if rank == 0 and not args.skip_check:
+        import oracle as O
+        for i in (0, k - 1):
+            want = O.bfs_csc(n, csc.col_ptrs, csc.rows, int(sources[i]))
+            if not np.array_equal(out[i].cpu().numpy().view(np.uint32), want):
+                raise SystemExit(f"MBFS levels differ from the oracle for source #{i}")
+    for _ in range(args.warmup):
+        mbfs_once()
+    barrier()
+    torch.cuda.synchronize()
+    times = []
+    with ClockSampler(dev) as clocks:
+        for _ in range(args.steps):
+            mbfs_once()
+            times.append(st.time)
+    barrier()
+    ms = sum(times) * 1e3
+    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms = float(ms_t.item())
+    value = mr * args.steps * world / (ms * 1e-3) / 1e9
+
+    # plain: one single-source BFS launch per source (same kernel family)
+    ws = Workspace(g)
+    stream = torch.cuda.Stream()
+    lv = torch.empty(n, dtype=torch.int32, device="cuda")
+    for s_ in sources[:8]:
+        ws.bfs_async(int(s_), lv.data_ptr(), stream.cuda_stream)
+    stream.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for s_ in sources:
+        ws.bfs_async(int(s_), lv.data_ptr(), stream.cuda_stream)
+    e1.record(stream)
+    stream.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+    plain = mr / (plain_ms * 1e-3) / 1e9
+
+    # e2e: public call with host output, one group (128 sources) per step
+    k_e = min(k, 128)
+    host = np.empty((k_e, n), dtype=np.uint32)
+    t0 = time.perf_counter()
+    e_steps = max(1, args.steps)
+    for _ in range(e_steps):
+        L.call("blest_mbfs", g._h, src.ctypes.data_as(L.P(L.u32)), k_e, host.ctypes.data, L.MEM_HOST,
+               C.byref(p), C.byref(st))
+    e_secs = time.perf_counter() - t0
+    mr_e = 0
+    hdeg = np.diff(csr.col_ptrs.astype(np.int64))
+    for i in range(k_e):
+        mr_e += int(hdeg[host[i] != 0xFFFFFFFF].sum()) // 2
+    e2e = mr_e * e_steps / e_secs / 1e9
+    peak, peak_kind = measured_peak()
+    out_bytes = 4 * k * n
+    achieved = out_bytes / (ms / args.steps * 1e-3) / 1e9
+    return {
+        "metric": "batched MBFS GTEPS (sum over sources of reached edges / batch time)",
+        "value": round(value, 3), "unit": "GTEPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generator; see config)",
+        "config": {"workload": args.workload, "description": desc, "n": n, "sources_per_step": k,
+                   "group_width": args.group_width, "reached_edges_per_step": mr,
+                   "plain_one_launch_per_source_gteps": round(plain, 3),
+                   "speedup_vs_plain": round(value / world / plain, 2),
+                   "output_bytes_per_step": out_bytes,
+                   "l2": "inputs and outputs larger than L2, no flush"},
+        "e2e": {"value": round(e2e, 3), "unit": "GTEPS", "h2d_bytes_per_step": 4 * k_e,
+                "d2h_bytes_per_step": 4 * k_e * n, "note": f"host output, {k_e} sources per step, host wall time"},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_source": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": out_bytes, "note": "output levels only (lower bound)"},
+        "clocks": clocks.summary(),
+    }
+
+
 def run_b200(args, rank, world):
     import torch
     import torch.distributed as dist
@@ -390,6 +503,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-check", action="store_true")
+    ap.add_argument("--group-width", type=int, default=128)
     args = ap.parse_args()
     if args.warmup < 3:
         log("warmup raised to 3 (minimum)")
@@ -403,6 +517,8 @@ def main():
     try:
         if args.impl == "reference":
             res = run_reference(args, rank, world)
+        elif WORKLOADS[args.workload][0] == "mbfs":
+            res = run_mbfs(args, rank, world)
         else:
             res = run_b200(args, rank, world)
         if rank == 0 and res is not None:

@@ -301,6 +301,7 @@ int blest_graph_destroy(blest_graph* g) {
         blest::workspace_free(g->default_ws->w);
         delete g->default_ws;
     }
+    blest::mbfs_scratch_free(g->mbfs);
     for (void* p : g->allocations) cudaFree(p);
     if (g->stream && g->owns_stream) cudaStreamDestroy(g->stream);
     delete g;

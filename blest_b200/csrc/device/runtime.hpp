@@ -54,6 +54,7 @@ struct blest_graph {
     cudaStream_t stream = nullptr;
     bool owns_stream = false;
     blest_workspace* default_ws = nullptr;
+    void* mbfs = nullptr;  // multi-source BFS scratch (mbfs.cu), grown on demand
 };
 
 struct blest_workspace {
@@ -87,5 +88,6 @@ void launch_bfs(const blest_graph* g, Workspace& w, uint32_t src, uint32_t* leve
 void launch_cc(const blest_graph* g, Workspace& w, uint32_t* labels, cudaStream_t s);
 
 int device_sm_count(int device);
+void mbfs_scratch_free(void* p);
 
 }  // namespace blest
