@@ -42,6 +42,7 @@ MEM_DEVICE = 1
 
 ORDER_AUTO, ORDER_NATURAL, ORDER_JACCARD, ORDER_RCM, ORDER_RANDOM, ORDER_DEGREE, ORDER_GORDER = range(7)
 DIR_AUTO, DIR_PUSH, DIR_PULL = 0, 1, 2
+QUERY_BFS, QUERY_CC = 0, 1
 TEST_CUDA_CORE, TEST_B1_MMA = 0, 1
 
 
@@ -110,6 +111,22 @@ class MbfsStats(C.Structure):
     _fields_ = [("time", f64), ("groups", u32), ("max_levels", u32), ("reached_degree_sum", u64)]
 
 
+class ServerParams(C.Structure):
+    _fields_ = [("memory_budget", u64), ("lanes", u32), ("max_batch", u32), ("queue_capacity", u32),
+                ("dry_run", i32)]
+
+
+class QueryResult(C.Structure):
+    _fields_ = [("status", i32), ("kind", i32), ("graph_id", u32), ("source", u32), ("batch_size", u32),
+                ("submit_s", f64), ("start_s", f64), ("done_s", f64)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", u64), ("completed", u64), ("rejected", u64), ("jobs", u64),
+                ("batched_requests", u64), ("p50_latency_s", f64), ("p99_latency_s", f64),
+                ("mean_latency_s", f64), ("busy_s", f64), ("peak_reserved_bytes", u64), ("memory_budget", u64)]
+
+
 class MbfsItem(C.Structure):
     _fields_ = [("graph", vp), ("sources", P(u32)), ("k", u32), ("levels_out", vp)]
 
@@ -169,6 +186,17 @@ _SIGS = {
     "blest_cc_relabel_dense": [P(u32), u32, P(u32), P(u32)],
     "blest_mbfs": [vp, P(u32), u32, vp, i32, P(MbfsParams), P(MbfsStats)],
     "blest_mbfs_batch": [P(MbfsItem), u32, i32, P(MbfsParams), vp, P(MbfsStats)],
+    "blest_mbfs_ws": [vp, P(u32), u32, vp, i32, P(MbfsParams), vp, P(MbfsStats)],
+    "blest_workspace_set_grid": [vp, u32],
+    "blest_server_create": [P(ServerParams), P(vp)],
+    "blest_server_add_graph": [vp, vp, P(u32)],
+    "blest_server_add_virtual_graph": [vp, u32, u64, P(u32)],
+    "blest_server_submit": [vp, u32, i32, u32, vp, P(u64)],
+    "blest_server_poll": [vp, u64, P(i32), P(QueryResult)],
+    "blest_server_wait": [vp, u64, f64, P(QueryResult)],
+    "blest_server_drain": [vp, f64],
+    "blest_server_stats_get": [vp, P(ServerStats)],
+    "blest_server_destroy": [vp],
 }
 
 fn = {}

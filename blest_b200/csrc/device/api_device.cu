@@ -161,6 +161,7 @@ void workspace_free(Workspace& w) {
     cudaFree(w.trace);
     for (auto& x : w.summary) cudaFree(x);
     cudaFree(w.heavy);
+    mbfs_scratch_free(w.mbfs);
     if (w.host_counters) cudaFreeHost(w.host_counters);
     if (w.ev_start) cudaEventDestroy(w.ev_start);
     if (w.ev_stop) cudaEventDestroy(w.ev_stop);
@@ -301,7 +302,6 @@ int blest_graph_destroy(blest_graph* g) {
         blest::workspace_free(g->default_ws->w);
         delete g->default_ws;
     }
-    blest::mbfs_scratch_free(g->mbfs);
     for (void* p : g->allocations) cudaFree(p);
     if (g->stream && g->owns_stream) cudaStreamDestroy(g->stream);
     delete g;
@@ -345,6 +345,13 @@ int blest_workspace_create(const blest_graph* g, blest_workspace** out) {
     });
     if (rc != BLEST_OK && ws) blest_workspace_destroy(ws);
     return rc;
+}
+
+int blest_workspace_set_grid(blest_workspace* ws, uint32_t blocks) {
+    return guarded([&] {
+        blest::require(ws, "null argument");
+        ws->w.grid_blocks = blocks;
+    });
 }
 
 int blest_workspace_destroy(blest_workspace* ws) {

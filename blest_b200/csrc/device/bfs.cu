@@ -637,7 +637,7 @@ namespace {
 
 template <bool ALIGNED, bool MMA, bool PARENTS>
 void launch_variant(const blest_graph* g, const dev::BfsArgs& args, int blocks_per_sm, int threads,
-                    cudaStream_t s) {
+                    uint32_t grid_cap, cudaStream_t s) {
     auto kern = dev::bfs_persistent_kernel<ALIGNED, MMA, PARENTS>;
     const size_t smem = 4ull * args.sum_words;
     BLEST_CUDA(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -645,7 +645,7 @@ void launch_variant(const blest_graph* g, const dev::BfsArgs& args, int blocks_p
     BLEST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxBlocks, kern, threads, smem));
     if (maxBlocks < 1) throw Error(BLEST_ERR_CUDA, "BFS kernel cannot be resident with this block size");
     const int bps = blocks_per_sm > 0 ? std::min(blocks_per_sm, maxBlocks) : maxBlocks;
-    const int grid = bps * g->sm_count;
+    const int grid = cooperative_grid(bps, g->sm_count, grid_cap);
     BLEST_CUDA(cudaMemsetAsync(args.ctr, 0, sizeof(dev::RunCounters), s));
     void* kargs[] = {(void*)&args};
     BLEST_CUDA(cudaLaunchCooperativeKernel((void*)kern, grid, threads, kargs, smem, s));
@@ -685,11 +685,11 @@ void launch_bfs(const blest_graph* g, Workspace& w, uint32_t src, uint32_t* leve
     const bool mma = p.slice_test == BLEST_TEST_B1_MMA;
     const bool par = parents != nullptr;
     if (mma) {
-        if (par) launch_variant<true, true, true>(g, a, p.blocks_per_sm, threads, s);
-        else launch_variant<true, true, false>(g, a, p.blocks_per_sm, threads, s);
+        if (par) launch_variant<true, true, true>(g, a, p.blocks_per_sm, threads, w.grid_blocks, s);
+        else launch_variant<true, true, false>(g, a, p.blocks_per_sm, threads, w.grid_blocks, s);
     } else {
-        if (par) launch_variant<false, false, true>(g, a, p.blocks_per_sm, threads, s);
-        else launch_variant<false, false, false>(g, a, p.blocks_per_sm, threads, s);
+        if (par) launch_variant<false, false, true>(g, a, p.blocks_per_sm, threads, w.grid_blocks, s);
+        else launch_variant<false, false, false>(g, a, p.blocks_per_sm, threads, w.grid_blocks, s);
     }
 }
 

@@ -285,7 +285,7 @@ void launch_cc(const blest_graph* g, Workspace& w, uint32_t* labels, cudaStream_
     int maxBlocks = 0;
     BLEST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxBlocks, dev::cc_persistent_kernel, threads, 0));
     if (maxBlocks < 1) throw Error(BLEST_ERR_CUDA, "CC kernel cannot be resident");
-    const int grid = maxBlocks * g->sm_count;
+    const int grid = cooperative_grid(maxBlocks, g->sm_count, w.grid_blocks);
     dev::cc_reset_kernel<<<1, 1, 0, s>>>(a);
     BLEST_CUDA(cudaGetLastError());
     dev::cc_init_kernel<<<g->sm_count * 4, 512, 0, s>>>(a);

@@ -386,7 +386,8 @@ void launch_mbfs(const blest_graph* g, blest::Workspace& w, MbfsScratch& sc, con
     const int bps = p.blocks_per_sm > 0 ? std::min(p.blocks_per_sm, maxBlocks) : maxBlocks;
     BLEST_CUDA(cudaMemsetAsync(a.ctr, 0, sizeof(dev::RunCounters), s));
     void* kargs[] = {(void*)&a};
-    BLEST_CUDA(cudaLaunchCooperativeKernel((void*)kern, bps * g->sm_count, threads, kargs, 0, s));
+    BLEST_CUDA(cudaLaunchCooperativeKernel((void*)kern, cooperative_grid(bps, g->sm_count, w.grid_blocks), threads,
+                                           kargs, 0, s));
 }
 
 }  // namespace
@@ -406,11 +407,12 @@ using blest::guarded;
 
 extern "C" {
 
-int blest_mbfs(blest_graph* g, const uint32_t* sources, uint32_t k, uint32_t* levels_out, int out_mem,
-               const blest_mbfs_params* params, blest_mbfs_stats* stats) {
+int blest_mbfs_ws(blest_workspace* ws, const uint32_t* sources, uint32_t k, uint32_t* levels_out, int out_mem,
+                  const blest_mbfs_params* params, void* stream, blest_mbfs_stats* stats) {
     return guarded([&] {
-        blest::require(g && sources && levels_out, "null argument");
+        blest::require(ws && sources && levels_out, "null argument");
         blest::require(out_mem == BLEST_MEM_HOST || out_mem == BLEST_MEM_DEVICE, "bad out_mem");
+        const blest_graph* g = ws->g;
         const uint32_t n = g->d.n;
         for (uint32_t i = 0; i < k; ++i)
             if (sources[i] >= n) throw blest::Error(BLEST_ERR_INVALID_ARG, "source vertex out of range");
@@ -420,10 +422,10 @@ int blest_mbfs(blest_graph* g, const uint32_t* sources, uint32_t k, uint32_t* le
         const uint32_t gw = p.group_width ? p.group_width : 128;
         blest::require(gw == 32 || gw == 64 || gw == 128, "group_width must be 32, 64 or 128");
         BLEST_CUDA(cudaSetDevice(g->device));
-        cudaStream_t s = g->stream;
-        blest::Workspace& w = g->default_ws->w;
-        if (!g->mbfs) g->mbfs = new blest::MbfsScratch;
-        blest::MbfsScratch& sc = *(blest::MbfsScratch*)g->mbfs;
+        cudaStream_t s = stream ? (cudaStream_t)stream : g->stream;
+        blest::Workspace& w = ws->w;
+        if (!w.mbfs) w.mbfs = new blest::MbfsScratch;
+        blest::MbfsScratch& sc = *(blest::MbfsScratch*)w.mbfs;
         blest::ensure(sc.sources, sc.sources_cap, k);
         BLEST_CUDA(cudaMemcpyAsync(sc.sources, sources, 4ull * k, cudaMemcpyHostToDevice, s));
         uint32_t* dl = levels_out;
@@ -454,6 +456,15 @@ int blest_mbfs(blest_graph* g, const uint32_t* sources, uint32_t k, uint32_t* le
             stats->reached_degree_sum = 0;
         }
     });
+}
+
+int blest_mbfs(blest_graph* g, const uint32_t* sources, uint32_t k, uint32_t* levels_out, int out_mem,
+               const blest_mbfs_params* params, blest_mbfs_stats* stats) {
+    if (!g) {
+        blest::set_last_error("null graph");
+        return BLEST_ERR_INVALID_ARG;
+    }
+    return blest_mbfs_ws(g->default_ws, sources, k, levels_out, out_mem, params, g->stream, stats);
 }
 
 int blest_mbfs_batch(const blest_mbfs_item* items, uint32_t count, int out_mem, const blest_mbfs_params* params,

@@ -38,6 +38,8 @@ struct Workspace {
     uint32_t sum_words = 0;                     // 32-bit words per summary
     uint4* heavy = nullptr;                     // pull: very long in-neighbour lists
     uint32_t heavy_cap = 0;
+    uint32_t grid_blocks = 0;                   // cap on cooperative grid size (0 = whole GPU)
+    void* mbfs = nullptr;                       // multi-source BFS scratch (mbfs.cu), grown on demand
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     uint64_t bytes = 0;
 };
@@ -54,7 +56,6 @@ struct blest_graph {
     cudaStream_t stream = nullptr;
     bool owns_stream = false;
     blest_workspace* default_ws = nullptr;
-    void* mbfs = nullptr;  // multi-source BFS scratch (mbfs.cu), grown on demand
 };
 
 struct blest_workspace {
@@ -89,5 +90,10 @@ void launch_cc(const blest_graph* g, Workspace& w, uint32_t* labels, cudaStream_
 
 int device_sm_count(int device);
 void mbfs_scratch_free(void* p);
+// Cooperative grid: occupancy maximum, optionally capped by the workspace.
+inline int cooperative_grid(int max_blocks_per_sm, int sm_count, uint32_t cap) {
+    const int full = max_blocks_per_sm * sm_count;
+    return cap && (int)cap < full ? (int)cap : full;
+}
 
 }  // namespace blest

@@ -219,6 +219,10 @@ int blest_graph_set_stream(blest_graph* g, void* stream);
  * concurrently running query on a graph. */
 int blest_workspace_create(const blest_graph* g, blest_workspace** out);
 int blest_workspace_destroy(blest_workspace* ws);
+/* Cap the cooperative grid of this workspace's kernels at `blocks` (0 = the
+ * whole GPU), so queries on different workspaces/streams can run side by
+ * side (the query server gives each executor lane a share of the SMs). */
+int blest_workspace_set_grid(blest_workspace* ws, uint32_t blocks);
 
 /* ---- single-source BFS -------------------------------------------------- */
 #define BLEST_DIR_AUTO 0       /* direction-optimising (push <-> pull) */
@@ -348,6 +352,9 @@ typedef struct blest_mbfs_stats {
 } blest_mbfs_stats;
 int blest_mbfs(blest_graph* g, const uint32_t* sources, uint32_t k, uint32_t* levels_out, int out_mem,
                const blest_mbfs_params* params, blest_mbfs_stats* stats);
+/* Same on an explicit workspace and stream (blocking). */
+int blest_mbfs_ws(blest_workspace* ws, const uint32_t* sources, uint32_t k, uint32_t* levels_out, int out_mem,
+                  const blest_mbfs_params* params, void* stream, blest_mbfs_stats* stats);
 
 /* Many graphs, many sources, one persistent launch. */
 typedef struct blest_mbfs_item {
@@ -358,6 +365,62 @@ typedef struct blest_mbfs_item {
 } blest_mbfs_item;
 int blest_mbfs_batch(const blest_mbfs_item* items, uint32_t count, int out_mem, const blest_mbfs_params* params,
                      void* stream, blest_mbfs_stats* stats);
+
+/* ======================================================================= */
+/*  Query server (continuous batching; no counterpart in the reference)     */
+/* ======================================================================= */
+/* BFS / CC requests on resident graphs are queued; whenever one of `lanes`
+ * executors (each a CUDA stream with its own workspaces and a share of the
+ * SMs) is free, the scheduler forms the next job from what is pending:
+ * BFS requests on one graph are coalesced (up to max_batch) into one
+ * multi-source BFS, CC requests on one graph share one run. A job is
+ * admitted when its device scratch fits the memory budget: the batch
+ * shrinks or the job waits for running jobs to finish; a request that can
+ * never fit is refused with BLEST_ERR_ADMISSION. Results land in the
+ * caller's host buffer (n uint32 levels or labels). Graphs stay owned by
+ * the caller and must outlive the server. */
+typedef struct blest_server blest_server;
+#define BLEST_QUERY_BFS 0
+#define BLEST_QUERY_CC 1
+typedef struct blest_server_params {
+    uint64_t memory_budget;   /* device bytes for job scratch; 0 = half the free memory */
+    uint32_t lanes;           /* concurrent executors; 0 = 4 */
+    uint32_t max_batch;       /* sources per multi-source batch, <= 128; 0 = 128 */
+    uint32_t queue_capacity;  /* pending requests; 0 = 2^20 (BLEST_ERR_BUSY beyond) */
+    int dry_run;              /* != 0: no GPU; jobs finish at once and out[0] = batch size
+                                 (exercises the scheduling logic) */
+} blest_server_params;
+typedef struct blest_query_result {
+    int status;               /* BLEST_OK or the error code of the request */
+    int kind;                 /* BLEST_QUERY_* */
+    uint32_t graph_id;
+    uint32_t source;
+    uint32_t batch_size;      /* requests served by the same GPU job */
+    double submit_s;          /* seconds since server start (host steady clock) */
+    double start_s;
+    double done_s;
+} blest_query_result;
+typedef struct blest_server_stats {
+    uint64_t submitted, completed, rejected;
+    uint64_t jobs;            /* GPU jobs run */
+    uint64_t batched_requests;/* requests served by a job of two or more */
+    double p50_latency_s, p99_latency_s, mean_latency_s;
+    double busy_s;            /* summed lane busy time */
+    uint64_t peak_reserved_bytes;
+    uint64_t memory_budget;
+} blest_server_stats;
+int blest_server_create(const blest_server_params* p, blest_server** out);
+int blest_server_add_graph(blest_server* s, blest_graph* g, uint32_t* graph_id);
+/* Dry-run servers only: a graph described by its size. */
+int blest_server_add_virtual_graph(blest_server* s, uint32_t n, uint64_t nnz, uint32_t* graph_id);
+int blest_server_submit(blest_server* s, uint32_t graph_id, int kind, uint32_t source, uint32_t* out_host,
+                        uint64_t* ticket);
+int blest_server_poll(blest_server* s, uint64_t ticket, int* done, blest_query_result* result);
+int blest_server_wait(blest_server* s, uint64_t ticket, double timeout_s, blest_query_result* result);
+/* Wait until every submitted request has finished or been refused. */
+int blest_server_drain(blest_server* s, double timeout_s);
+int blest_server_stats_get(blest_server* s, blest_server_stats* out);
+int blest_server_destroy(blest_server* s);
 
 #ifdef __cplusplus
 }

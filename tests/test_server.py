@@ -1,0 +1,135 @@
+"""Query server: scheduling logic on CPU (dry-run mode) and, on the GPU,
+results identical alone and in a concurrent mix."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from blest_b200 import BlestError
+from blest_b200.server import Server
+
+
+def test_dry_run_coalesces_bfs_and_shares_cc():
+    srv = Server(lanes=1, max_batch=128, dry_run=True)
+    g0 = srv.add_virtual_graph(1000)
+    g1 = srv.add_virtual_graph(5000)
+    # one lane: while the first job is being formed the others queue up
+    tickets = [srv.submit_bfs(g0, i) for i in range(300)]
+    tickets += [srv.submit_cc(g1) for _ in range(5)]
+    tickets += [srv.submit_bfs(g1, i) for i in range(3)]
+    srv.drain(30)
+    infos = [t.info() for t in tickets]
+    assert all(i.status == 0 for i in infos)
+    bfs0 = [i.batch_size for i in infos[:300]]
+    assert max(bfs0) <= 128 and sum(1 for b in bfs0 if b > 1) > 0
+    cc = [i.batch_size for i in infos[300:305]]
+    assert sum(1.0 / b for b in cc) < 5  # CC requests pending together shared runs
+    # batch size recorded in out[0] by the dry executor
+    assert all(int(t.out[0]) == i.batch_size for t, i in zip(tickets, infos))
+    st = srv.stats()
+    assert st["completed"] == 308 and st["rejected"] == 0
+    assert st["jobs"] < 308
+    assert st["p99_latency_s"] >= st["p50_latency_s"] >= 0
+
+
+def test_dry_run_admission_shrinks_batches_and_refuses_the_impossible():
+    n = 1 << 20
+    # a 2-source batch needs 3*n*4 (state) + 2*4*n (levels) bytes = 20 MiB
+    srv = Server(lanes=2, max_batch=128, memory_budget=21 << 20, dry_run=True)
+    g = srv.add_virtual_graph(n)
+    ts = [srv.submit_bfs(g, i) for i in range(64)]
+    srv.drain(30)
+    infos = [t.info() for t in ts]
+    assert all(i.status == 0 for i in infos)
+    assert max(i.batch_size for i in infos) <= 2
+    st = srv.stats()
+    assert st["peak_reserved_bytes"] <= 21 << 20
+    # budget 0 bytes beyond resident: single BFS needs no scratch, batches cannot form
+    srv2 = Server(lanes=1, memory_budget=1, dry_run=True)
+    g2 = srv2.add_virtual_graph(n)
+    ts2 = [srv2.submit_bfs(g2, i) for i in range(10)]
+    srv2.drain(30)
+    assert all(t.info().batch_size == 1 for t in ts2)
+
+
+def test_dry_run_validation_and_threads():
+    srv = Server(lanes=3, dry_run=True)
+    g = srv.add_virtual_graph(100)
+    with pytest.raises(BlestError):
+        srv.submit_bfs(g, 100)  # source out of range
+    with pytest.raises(BlestError):
+        srv.submit_bfs(7, 0)  # unknown graph
+    out = []
+
+    def client(seed):
+        rng = np.random.default_rng(seed)
+        for _ in range(200):
+            out.append(srv.submit_bfs(g, int(rng.integers(0, 100))))
+            if rng.random() < 0.1:
+                time.sleep(0.0005)
+
+    th = [threading.Thread(target=client, args=(i,)) for i in range(4)]
+    [t.start() for t in th]
+    [t.join() for t in th]
+    srv.drain(30)
+    assert srv.stats()["completed"] == 800
+    assert all(t.done() for t in out)
+
+
+@pytest.mark.gpu
+def test_results_equal_alone_and_in_the_mix(gpu):
+    import oracle as O
+    from blest_b200 import Csc, Graph
+    from graphs import prepared
+    graphs = []
+    for make in (lambda: Csc.rmat(14, 16, seed=1, permute_seed=2), lambda: Csc.grid(90, 70, 0.05, 0.01, seed=3),
+                 lambda: Csc.er(6000, 30000, seed=5)):
+        csc, bvss, csr = prepared(make(), "auto", 4096)
+        graphs.append((csc, Graph(bvss, csr)))
+    srv = Server(lanes=4, max_batch=64)
+    gids = [srv.add_graph(g) for _, g in graphs]
+    rng = np.random.default_rng(11)
+    reqs = []
+    for i in range(400):
+        gi = int(rng.integers(0, len(graphs)))
+        if rng.random() < 0.2:
+            reqs.append((gi, "cc", None, srv.submit_cc(gids[gi])))
+        else:
+            s = int(rng.integers(0, graphs[gi][0].n))
+            reqs.append((gi, "bfs", s, srv.submit_bfs(gids[gi], s)))
+        if rng.random() < 0.05:
+            time.sleep(0.001)
+    srv.drain(120)
+    batched = 0
+    for gi, kind, s, t in reqs:
+        csc, g = graphs[gi]
+        info = t.info()
+        assert info.status == 0
+        batched += info.batch_size > 1
+        if kind == "bfs":
+            alone, _, _ = g.bfs(s)
+            np.testing.assert_array_equal(t.out, alone)
+            np.testing.assert_array_equal(t.out, O.bfs_csc(csc.n, csc.col_ptrs, csc.rows, s))
+        else:
+            alone, _ = g.cc()
+            np.testing.assert_array_equal(t.out, alone)
+    assert batched > 0  # some requests were coalesced
+    st = srv.stats()
+    assert st["completed"] == 400 and st["p99_latency_s"] > 0
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_request_that_never_fits_is_refused(gpu):
+    from blest_b200 import Csc, Graph
+    from graphs import prepared
+    csc, bvss, csr = prepared(Csc.rmat(12, 8, seed=1, permute_seed=1), "jaccard", 1024)
+    g = Graph(bvss, csr)
+    srv = Server(lanes=1, max_batch=128, memory_budget=1)
+    gid = srv.add_graph(g)
+    ts = [srv.submit_bfs(gid, i) for i in range(40)]
+    srv.drain(60)
+    # batches cannot be admitted; single-source queries need no extra scratch
+    assert all(t.info().status == 0 and t.info().batch_size == 1 for t in ts)
+    srv.close()
