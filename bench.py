@@ -45,6 +45,9 @@ WORKLOADS = {
                  "2D 4096x4096 grid, 5% edges deleted, 0.1% shortcuts, RCM, 32 seeded sources"),
     "er25": ("bfs", ("er", 25, 32), "rcm", 0, 32, "Erdos-Renyi 2^25 vertices avg degree 32, RCM, 32 sources"),
     "cc_rmat24": ("cc", ("rmat", 24, 16), "jaccard", 65536, 0, "connected components, RMAT scale 24"),
+    "serving": ("serving", None, None, 0, 0,
+                "query server: resident graphs RMAT 18/20/22, grid 1024^2, ER 2^22 deg 16; Poisson arrivals, "
+                "80% BFS (uniform seeded source) / 20% CC, graph uniform; rate sweep"),
     "mbfs_rmat22": ("mbfs", ("rmat", 22, 16), "jaccard", 65536, 1024,
                     "multi-source BFS, RMAT scale 22 ef 16, Jaccard window 65536, 1024 seeded sources "
                     "in bit-packed groups of 128"),
@@ -300,6 +303,146 @@ def run_mbfs(args, rank, world):
     }
 
 
+SERVING_GRAPHS = [
+    ("rmat18", ("rmat", 18, 16), "jaccard"), ("rmat20", ("rmat", 20, 16), "jaccard"),
+    ("rmat22", ("rmat", 22, 16), "jaccard"), ("grid1024", ("grid", 1024, 1024), "rcm"),
+    ("er22", ("er", 22, 16), "rcm"),
+]
+SERVING_GRAPHS_FULL = SERVING_GRAPHS[:3] + [("rmat24", ("rmat", 24, 16), "jaccard"), SERVING_GRAPHS[3],
+                                            ("grid4096", ("grid", 4096, 4096), "rcm"), SERVING_GRAPHS[4],
+                                            ("er24", ("er", 24, 32), "rcm")]
+
+
+def build_graph(gen, order):
+    from blest_b200 import Bvss, Csc
+    if gen[0] == "rmat":
+        csc = Csc.rmat(gen[1], gen[2], 0.57, 0.19, 0.19, seed=SEED, permute_seed=SEED)
+    elif gen[0] == "grid":
+        csc = Csc.grid(gen[1], gen[2], 0.05, 0.001, seed=SEED)
+    else:
+        n = 1 << gen[1]
+        csc = Csc.er(n, n * gen[2] // 2, seed=SEED)
+    csc.reorder(order, window=65536)
+    return csc, Bvss.build(csc)
+
+
+def run_serving(args, rank, world):
+    """Open-loop Poisson load on the query server, swept over arrival rates."""
+    import threading
+    import torch
+    import blest_b200
+    from blest_b200 import Graph
+    from blest_b200.server import Server
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    blest_b200.init(dev)
+    specs = SERVING_GRAPHS_FULL if args.serving_full else SERVING_GRAPHS
+    graphs = []
+    for name, gen, order in specs:
+        t0 = time.time()
+        csc, bvss = build_graph(gen, order)
+        g = Graph(bvss, csc)
+        srcs = csc.sample_sources(1024, SEED)
+        # reached undirected edges per pool source, from multi-source BFS
+        deg = torch.from_numpy(np.diff(csc.col_ptrs.astype(np.int64))).cuda()
+        lv = torch.empty((128, csc.n), dtype=torch.int32, device="cuda")
+        mr = []
+        for i in range(0, len(srcs), 128):
+            chunk = np.ascontiguousarray(srcs[i:i + 128], dtype=np.uint32)
+            import ctypes as C
+            from blest_b200 import _lib as L
+            L.call("blest_mbfs", g._h, chunk.ctypes.data_as(L.P(L.u32)), chunk.size, lv.data_ptr(), L.MEM_DEVICE,
+                   None, None)
+            mr += ((lv[:chunk.size] != -1).to(torch.int64) * deg).sum(1).div(2, rounding_mode="floor").tolist()
+        del lv
+        graphs.append((name, csc, g, np.array(mr, dtype=np.int64), srcs))
+        log(f"[serving] {name}: n={csc.n} nnz={csc.nnz} ({time.time() - t0:.1f}s)")
+    # pinned result buffers, recycled once a result has been consumed
+    import queue as qmod
+    pools = []
+    for _, csc, _, _, _ in graphs:
+        q = qmod.Queue()
+        for _ in range(args.buffers):
+            q.put(torch.empty(csc.n, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32))
+        pools.append(q)
+    rates = [float(r) for r in args.rates.split(",")]
+    rng = np.random.default_rng(SEED)
+    sweep = []
+    for lam in rates:
+        srv = Server(lanes=args.lanes, max_batch=128)
+        gids = [srv.add_graph(g) for _, _, g, _, _ in graphs]
+        nreq = int(min(args.requests, max(50, lam * args.seconds)))
+        gaps = rng.exponential(1.0 / lam, nreq)
+        kinds = rng.random(nreq) < 0.8
+        which = rng.integers(0, len(graphs), nreq)
+        tickets = []
+        edges = [0]
+        lock = threading.Lock()
+
+        def consume(queue):
+            while True:
+                item = queue.pop(0) if queue else None
+                if item is None:
+                    if done_flag[0] and not queue:
+                        return
+                    time.sleep(0.0005)
+                    continue
+                t, gi, si = item
+                t.result(600)
+                if si >= 0:
+                    with lock:
+                        edges[0] += int(graphs[gi][3][si])
+                pools[gi].put(t.out)
+                t.out = None
+
+        queue = []
+        done_flag = [False]
+        cons = threading.Thread(target=consume, args=(queue,))
+        cons.start()
+        t_start = time.perf_counter()
+        due = t_start
+        for i in range(nreq):
+            due += gaps[i]
+            while time.perf_counter() < due:
+                pass
+            gi = int(which[i])
+            buf = pools[gi].get()
+            si = -1
+            if kinds[i]:
+                src = graphs[gi][4]
+                si = int(rng.integers(0, len(src)))
+                t = srv.submit_bfs(gids[gi], int(src[si]), out=buf)
+            else:
+                t = srv.submit_cc(gids[gi], out=buf)
+            tickets.append(t)
+            queue.append((t, gi, si))
+        srv.drain(600)
+        wall = time.perf_counter() - t_start
+        done_flag[0] = True
+        cons.join()
+        st = srv.stats()
+        sweep.append({"rate_per_s": lam, "requests": nreq, "wall_s": round(wall, 3),
+                      "throughput_per_s": round(nreq / wall, 1),
+                      "p50_ms": round(st["p50_latency_s"] * 1e3, 3), "p99_ms": round(st["p99_latency_s"] * 1e3, 3),
+                      "mean_ms": round(st["mean_latency_s"] * 1e3, 3), "jobs": st["jobs"],
+                      "batched_requests": st["batched_requests"], "rejected": st["rejected"],
+                      "bfs_gteps": round(edges[0] / wall / 1e9, 3)})
+        log(f"[serving] rate {lam}/s: {sweep[-1]}")
+        srv.close()
+    head = sweep[min(1, len(sweep) - 1)]
+    return {
+        "metric": "serving p50 latency (ms) at the sweep's second rate; p50/p99 and GTEPS per rate in config.sweep",
+        "value": head["p50_ms"], "unit": "ms", "n_gpus": 1, "steps": len(sweep), "warmup": 0,
+        "ms_per_step": None, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded generators; Poisson arrivals from a fixed seed)",
+        "config": {"workload": "serving", "description": WORKLOADS["serving"][5],
+                   "graphs": [x[0] for x in graphs], "lanes": args.lanes, "max_batch": 128, "sweep": sweep},
+        "e2e": {"value": head["p50_ms"], "unit": "ms", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                "note": "latency measured from submit to result in host memory"},
+    }
+
+
 def run_b200(args, rank, world):
     import torch
     import torch.distributed as dist
@@ -504,6 +647,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-check", action="store_true")
     ap.add_argument("--group-width", type=int, default=128)
+    ap.add_argument("--rates", default="100,1000,10000,50000")
+    ap.add_argument("--requests", type=int, default=3000)
+    ap.add_argument("--seconds", type=float, default=2.0)
+    ap.add_argument("--lanes", type=int, default=4)
+    ap.add_argument("--serving-full", action="store_true")
+    ap.add_argument("--buffers", type=int, default=192)
     args = ap.parse_args()
     if args.warmup < 3:
         log("warmup raised to 3 (minimum)")
@@ -519,6 +668,8 @@ def main():
             res = run_reference(args, rank, world)
         elif WORKLOADS[args.workload][0] == "mbfs":
             res = run_mbfs(args, rank, world)
+        elif WORKLOADS[args.workload][0] == "serving":
+            res = run_serving(args, rank, world) if rank == 0 else None
         else:
             res = run_b200(args, rank, world)
         if rank == 0 and res is not None:

@@ -640,7 +640,10 @@ void launch_variant(const blest_graph* g, const dev::BfsArgs& args, int blocks_p
                     uint32_t grid_cap, cudaStream_t s) {
     auto kern = dev::bfs_persistent_kernel<ALIGNED, MMA, PARENTS>;
     const size_t smem = 4ull * args.sum_words;
-    BLEST_CUDA(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // Always the same (maximum) value: calls for graphs of different sizes
+    // may run concurrently from several threads.
+    BLEST_CUDA(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kSummaryMaxBytes));
     int maxBlocks = 0;
     BLEST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxBlocks, kern, threads, smem));
     if (maxBlocks < 1) throw Error(BLEST_ERR_CUDA, "BFS kernel cannot be resident with this block size");
@@ -741,7 +744,8 @@ template <bool PARENTS>
 void noalloc_launch(const dev::BfsArgs& a, int sms, cudaStream_t s) {
     auto kern = dev::bfs_persistent_kernel<false, false, PARENTS>;
     const size_t smem = 4ull * a.sum_words;
-    BLEST_CUDA(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    BLEST_CUDA(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kSummaryMaxBytes));
     int maxBlocks = 0;
     BLEST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxBlocks, kern, 512, smem));
     if (maxBlocks < 1) throw Error(BLEST_ERR_CUDA, "BFS kernel cannot be resident");

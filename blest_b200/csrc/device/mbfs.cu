@@ -392,6 +392,13 @@ void launch_mbfs(const blest_graph* g, blest::Workspace& w, MbfsScratch& sc, con
 
 }  // namespace
 
+void mbfs_reserve(Workspace& w, uint32_t n, uint32_t words) {
+    if (!w.mbfs) w.mbfs = new MbfsScratch;
+    MbfsScratch& sc = *(MbfsScratch*)w.mbfs;
+    ensure(sc.state, sc.state_words, 3ull * n * words);
+    ensure(sc.sources, sc.sources_cap, 128);
+}
+
 void mbfs_scratch_free(void* p) {
     MbfsScratch* sc = (MbfsScratch*)p;
     if (!sc) return;

@@ -90,6 +90,8 @@ void launch_cc(const blest_graph* g, Workspace& w, uint32_t* labels, cudaStream_
 
 int device_sm_count(int device);
 void mbfs_scratch_free(void* p);
+// Allocate the multi-source BFS state of `words` 32-bit words per vertex now.
+void mbfs_reserve(Workspace& w, uint32_t n, uint32_t words);
 // Cooperative grid: occupancy maximum, optionally capped by the workspace.
 inline int cooperative_grid(int max_blocks_per_sm, int sm_count, uint32_t cap) {
     const int full = max_blocks_per_sm * sm_count;

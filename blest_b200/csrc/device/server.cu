@@ -27,6 +27,7 @@
 #include <mutex>
 #include <thread>
 #include <unordered_map>
+#include <string>
 #include <vector>
 
 #include "../host/errors.hpp"
@@ -48,6 +49,7 @@ struct Request {
     uint32_t batch = 0;
     double submit = 0, start = 0, done_t = 0;
     bool done = false;
+    std::string error;
 };
 
 struct GraphEntry {
@@ -110,11 +112,12 @@ uint64_t job_bytes(const GraphEntry& ge, int kind, uint32_t k) {
     return 3ull * ge.n * 4 * words + 4ull * k * ge.n;  // MBFS state + staged levels
 }
 
-void finish(blest_server* s, Job& job, int status, double start) {
+void finish(blest_server* s, Job& job, int status, const std::string& err, double start) {
     const double t = now(s);
     std::lock_guard<std::mutex> lk(s->mu);
     for (Request* r : job.reqs) {
         r->status = status;
+        r->error = err;
         r->start = start;
         r->done_t = t;
         r->batch = (uint32_t)job.reqs.size();
@@ -185,7 +188,7 @@ void lane_main(blest_server* s, Lane* lane) {
         }
         const double start = now(s);
         const int rc = run_job(s, *lane, *job);
-        finish(s, *job, rc, start);
+        finish(s, *job, rc, rc == BLEST_OK ? std::string() : std::string(blest_last_error()), start);
         {
             std::lock_guard<std::mutex> lk(s->mu);
             lane->busy = false;
@@ -318,7 +321,18 @@ static int add_graph(blest_server* s, blest_graph* g, uint32_t n, uint64_t nnz, 
         ge.n = n;
         ge.nnz = nnz;
         s->graphs.push_back(ge);
-        for (auto& l : s->lanes) l->ws.push_back(nullptr);
+        for (auto& l : s->lanes) {
+            blest_workspace* ws = nullptr;
+            if (g) {
+                // one workspace per lane, created now so no request pays for
+                // device allocation; its cooperative grids get the lane's share
+                const int rc = blest_workspace_create(g, &ws);
+                if (rc != BLEST_OK) throw blest::Error(rc, blest_last_error());
+                blest_workspace_set_grid(ws, s->lane_grid);
+                blest::mbfs_reserve(ws->w, n, 4);
+            }
+            l->ws.push_back(ws);
+        }
         *id = (uint32_t)(s->graphs.size() - 1);
     });
 }
@@ -397,7 +411,8 @@ int blest_server_wait(blest_server* s, uint64_t ticket, double timeout_s, blest_
         const bool ok = s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] { return r->done; });
         if (!ok) throw blest::Error(BLEST_ERR_BUSY, "timed out waiting for the request");
         fill_result(*r, result);
-        if (r->status != BLEST_OK) throw blest::Error(r->status, "request failed");
+        if (r->status != BLEST_OK)
+            throw blest::Error(r->status, "request failed: " + (r->error.empty() ? std::string("refused") : r->error));
     });
 }
 

@@ -91,17 +91,20 @@ class Server:
         g = self._graphs.get(gid, 1)  # unknown ids are refused by the library
         return g if isinstance(g, int) else g.n
 
-    def _submit(self, gid: int, kind: int, source: int) -> Ticket:
-        out = np.empty(self._n(gid), dtype=np.uint32)
+    def _submit(self, gid: int, kind: int, source: int, out: np.ndarray | None = None) -> Ticket:
+        if out is None:
+            out = np.empty(self._n(gid), dtype=np.uint32)
+        assert out.dtype == np.uint32 and out.size >= self._n(gid) and out.flags.c_contiguous
         t = L.u64()
         L.call("blest_server_submit", self._h, gid, kind, source, out.ctypes.data, C.byref(t))
         return Ticket(self, t.value, out)
 
-    def submit_bfs(self, gid: int, source: int) -> Ticket:
-        return self._submit(gid, L.QUERY_BFS, source)
+    def submit_bfs(self, gid: int, source: int, out: np.ndarray | None = None) -> Ticket:
+        """`out`: optional uint32[n] result buffer (e.g. pinned memory)."""
+        return self._submit(gid, L.QUERY_BFS, source, out)
 
-    def submit_cc(self, gid: int) -> Ticket:
-        return self._submit(gid, L.QUERY_CC, 0)
+    def submit_cc(self, gid: int, out: np.ndarray | None = None) -> Ticket:
+        return self._submit(gid, L.QUERY_CC, 0, out)
 
     def drain(self, timeout_s: float = 600.0) -> None:
         L.call("blest_server_drain", self._h, timeout_s)
