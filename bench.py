@@ -214,7 +214,14 @@ def run_mbfs(args, rank, world):
     deg = torch.from_numpy(np.diff(csr.col_ptrs.astype(np.int64))).cuda()
     out = torch.empty((k, n), dtype=torch.int32, device="cuda")
     src = np.ascontiguousarray(sources, dtype=np.uint32)
-    p = L.MbfsParams(args.group_width, 0, 0)
+    tuned = None
+    if not args.no_autotune_mbfs:
+        from blest_b200.autotune import tune_mbfs
+        tuned, table = tune_mbfs(g, sources)
+        log(f"[autotune] mbfs best {tuned} ({table[0]['seconds'] * 1e3:.2f} ms; worst {table[-1]['seconds'] * 1e3:.2f})")
+        p = L.MbfsParams(tuned["group_width"], tuned["blocks_per_sm"], 0)
+    else:
+        p = L.MbfsParams(args.group_width, 0, 0)
     st = L.MbfsStats()
     barrier = (lambda: dist.barrier()) if world > 1 else (lambda: None)
 
@@ -288,7 +295,8 @@ def run_mbfs(args, rank, world):
         "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generator; see config)",
         "config": {"workload": args.workload, "description": desc, "n": n, "sources_per_step": k,
-                   "group_width": args.group_width, "reached_edges_per_step": mr,
+                   "group_width": p.group_width, "blocks_per_sm": p.blocks_per_sm or "max",
+                   "autotuned": tuned is not None, "reached_edges_per_step": mr,
                    "plain_one_launch_per_source_gteps": round(plain, 3),
                    "speedup_vs_plain": round(value / world / plain, 2),
                    "output_bytes_per_step": out_bytes,
@@ -465,6 +473,14 @@ def run_b200(args, rank, world):
     out = torch.empty(n, dtype=torch.int32, device="cuda")
     barrier = (lambda: dist.barrier()) if world > 1 else (lambda: None)
 
+    params = None
+    tuned = None
+    if args.autotune:
+        from blest_b200.autotune import tune_bfs
+        params, table = tune_bfs(g, sources)
+        tuned = table[0]["params"]
+        log(f"[autotune] best {tuned}: {table[0]['seconds'] * 1e3:.3f} ms/BFS "
+            f"(worst {table[-1]['seconds'] * 1e3:.3f})")
     # Reference answers for m_R (levels are deterministic), outside timing.
     host_lv = np.empty(n, dtype=np.uint32)
     mr, algo = [], []
@@ -487,7 +503,7 @@ def run_b200(args, rank, world):
         for i, s in enumerate(sources):
             if events is not None:
                 events[i][0].record(stream)
-            ws.bfs_async(int(s), out.data_ptr(), sptr)
+            ws.bfs_async(int(s), out.data_ptr(), sptr, params=params)
             if events is not None:
                 events[i][1].record(stream)
 
@@ -526,7 +542,7 @@ def run_b200(args, rank, world):
     e0.record(stream)
     for _ in range(args.steps):
         for s in sources:
-            ws.bfs(int(s), pin_np, sptr)
+            ws.bfs(int(s), pin_np, sptr, params=params)
     e1.record(stream)
     stream.synchronize()
     e2e_ms_t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
@@ -550,7 +566,8 @@ def run_b200(args, rank, world):
                    "reached_edges_per_step": edges_per_step, "bvss_slices": int(info.no_slices),
                    "graph_bytes_hbm": int(info.device_bytes_graph),
                    "l2": "inputs larger than L2 (BVSS+CSR in HBM), no flush",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "bfs_params": tuned or "defaults (alpha 14, beta 24, occupancy grid, CUDA-core slice test)"},
         "e2e": {"value": round(e2e, 3), "unit": "GTEPS", "h2d_bytes_per_step": 4 * int(len(sources)),
                 "d2h_bytes_per_step": 4 * n * int(len(sources))},
         "gpu_launches": int(len(sources)) * args.steps,
@@ -653,6 +670,8 @@ def main():
     ap.add_argument("--lanes", type=int, default=4)
     ap.add_argument("--serving-full", action="store_true")
     ap.add_argument("--buffers", type=int, default=192)
+    ap.add_argument("--autotune", action="store_true", help="tune BFS launch parameters before timing")
+    ap.add_argument("--no-autotune-mbfs", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         log("warmup raised to 3 (minimum)")

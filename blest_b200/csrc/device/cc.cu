@@ -113,17 +113,6 @@ __global__ void cc_seed_queue_kernel(CcArgs a) {
     }
 }
 
-__global__ void cc_reset_kernel(CcArgs a) {
-    RunCounters* c = a.ctr;
-    c->bar_count = 0;
-    c->bar_gen = 0;
-    c->error = 0;
-    c->iterations = 0;
-    c->discovered = 0;
-    for (int i = 0; i < 4; ++i) a.qctr[i] = 0;
-    a.qctr[4] = 0;  // label updates, cumulative
-}
-
 __device__ __forceinline__ uint32_t cc_find_owner(const uint32_t* q_off, uint32_t lo, uint32_t hi, uint32_t pos) {
     const uint32_t lane = threadIdx.x & 31;
     while (hi - lo > 32) {
@@ -286,8 +275,7 @@ void launch_cc(const blest_graph* g, Workspace& w, uint32_t* labels, cudaStream_
     BLEST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxBlocks, dev::cc_persistent_kernel, threads, 0));
     if (maxBlocks < 1) throw Error(BLEST_ERR_CUDA, "CC kernel cannot be resident");
     const int grid = cooperative_grid(maxBlocks, g->sm_count, w.grid_blocks);
-    dev::cc_reset_kernel<<<1, 1, 0, s>>>(a);
-    BLEST_CUDA(cudaGetLastError());
+    BLEST_CUDA(cudaMemsetAsync(w.counters, 0, sizeof(dev::RunCounters), s));
     dev::cc_init_kernel<<<g->sm_count * 4, 512, 0, s>>>(a);
     BLEST_CUDA(cudaGetLastError());
     dev::cc_seed_queue_kernel<<<g->sm_count * 4, 512, 0, s>>>(a);

@@ -41,7 +41,12 @@ struct DevGraph {
     const uint32_t* has_in;     // ceil(n/32) words: bit v = v has an in-neighbour (may be null)
 };
 
-// Counters of one BFS/CC run (zeroed by the init kernel).
+// Grid barrier geometry: blocks arrive in groups of kBarrierGroup on
+// separate counters; the last block of each group arrives at the root.
+constexpr uint32_t kBarrierGroup = 16;
+constexpr uint32_t kBarrierMaxGroups = 64;
+
+// Counters of one BFS/CC run (zeroed before every run).
 struct RunCounters {
     unsigned long long queue;       // packed entries/units, cumulative
     unsigned long long discovered;  // vertices discovered, cumulative
@@ -63,6 +68,9 @@ struct RunCounters {
     unsigned int pad2[2];
     // CC: packed queue counters of 4 iteration slots + cumulative label updates.
     unsigned long long aux[8];
+    // Hierarchical grid barrier: one arrival counter per group of
+    // kBarrierGroup blocks, each on its own 128-byte line, plus the root.
+    unsigned int bar_group[kBarrierMaxGroups * 32];
 };
 
 __device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
@@ -98,18 +106,28 @@ __device__ __forceinline__ void set_error(RunCounters* c, uint32_t code) { atomi
 // Grid-wide barrier for a cooperative (co-resident) launch, with a bounded
 // wait: a block that waits longer than kBarrierTimeoutNs records
 // BLEST_ERR_BARRIER_TIMEOUT and leaves; every caller then sees the error and
-// returns, so no wait is unbounded. Before releasing the other blocks, the
-// last arriving block copies the run counters into the snapshot slot of
-// this barrier's parity, so all blocks read identical values afterwards
-// even while others already update the live counters.
+// returns, so no wait is unbounded. Arrival is two-level (a counter per
+// group of kBarrierGroup blocks, then the root) so that no single address
+// takes more than ~max(kBarrierGroup, groups) atomics. Before releasing the
+// other blocks, the last arriving block copies the run counters into the
+// snapshot slot of this barrier's parity, so all blocks read identical
+// values afterwards even while others already update the live counters.
 // Returns false if the run has an error recorded.
 __device__ __forceinline__ bool grid_barrier(RunCounters* c, uint32_t parity) {
     __syncthreads();
     if (threadIdx.x == 0) {
         const uint32_t gen = ld_acquire(&c->bar_gen);
         __threadfence();
-        const uint32_t arrived = atomicAdd(&c->bar_count, 1u);
-        if (arrived == gridDim.x - 1) {
+        const uint32_t grp = blockIdx.x / kBarrierGroup;
+        const uint32_t groups = (gridDim.x + kBarrierGroup - 1) / kBarrierGroup;
+        const uint32_t gsize = min(kBarrierGroup, gridDim.x - grp * kBarrierGroup);
+        bool root = false;
+        if (atomicAdd(&c->bar_group[grp * 32], 1u) == gsize - 1) {
+            c->bar_group[grp * 32] = 0;  // nobody touches it again before the release
+            __threadfence();
+            root = atomicAdd(&c->bar_count, 1u) == groups - 1;
+        }
+        if (root) {
             c->snap_queue[parity] = ld_relaxed64(&c->queue);
             c->snap_discovered[parity] = ld_relaxed64(&c->discovered);
             c->snap_degree[parity] = ld_relaxed64(&c->degree);
@@ -124,7 +142,7 @@ __device__ __forceinline__ bool grid_barrier(RunCounters* c, uint32_t parity) {
                     set_error(c, BLEST_ERR_BARRIER_TIMEOUT);
                     break;
                 }
-                __nanosleep(40);
+                if (spins > 64) __nanosleep(32);
             }
             __threadfence();
         }

@@ -406,7 +406,7 @@ class Workspace:
                         st.pull_levels, st.reached_degree_sum)
 
     def bfs(self, source: int, levels_out: np.ndarray, stream: int = 0, params: L.BfsParams | None = None):
-        """Blocking BFS into a host array (pinned or pageable)."""
+        """Blocking BFS into a host array (pinned or pageable); returns BfsStats."""
         st = L.BfsStats()
         L.call("blest_bfs_ws", self._h, source, levels_out.ctypes.data, None, L.MEM_HOST,
                C.byref(params) if params is not None else None, stream, 0, C.byref(st))
