@@ -583,6 +583,100 @@ def run_b200(args, rank, world):
     return result
 
 
+def run_cc(args, rank, world):
+    """Connected components by BVSS label propagation: ms per full CC run
+    (labels = minimum vertex id of the component), device output; e2e adds
+    the labels' device->host copy into pinned memory."""
+    import torch
+    import torch.distributed as dist
+    import blest_b200
+    from blest_b200 import Graph, Workspace
+    from blest_b200._lib import MEM_HOST
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    blest_b200.init(dev)
+    kind, gen, order, window, nsrc, desc = WORKLOADS[args.workload]
+    csc, bvss, csr, _ = prepare(args.workload, Path(args.cache), rank, world)
+    g = Graph(bvss, csr)
+    info = g.info()
+    n = csc.n
+    barrier = (lambda: dist.barrier()) if world > 1 else (lambda: None)
+    ws = Workspace(g)
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+    out = torch.empty(n, dtype=torch.int32, device="cuda")
+    lab, st0 = g.cc()
+    if rank == 0 and not args.skip_check:
+        import oracle as O
+        if not np.array_equal(lab, O.cc_csc(n, csc.col_ptrs, csc.rows)):
+            raise SystemExit("CC labels differ from the oracle")
+    for _ in range(args.warmup):
+        ws.cc(out.data_ptr(), sptr)
+    kern = []
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clocks:
+        t0.record(stream)
+        for _ in range(args.steps):
+            kern.append(ws.cc(out.data_ptr(), sptr).time)
+        t1.record(stream)
+        stream.synchronize()
+    barrier()
+    ms_t = torch.tensor([t0.elapsed_time(t1) / args.steps], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms = float(ms_t.item())
+
+    pinned = torch.empty(n, dtype=torch.int32, pin_memory=True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ws.cc(pinned.data_ptr(), sptr, MEM_HOST)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        ws.cc(pinned.data_ptr(), sptr, MEM_HOST)
+    e1.record(stream)
+    stream.synchronize()
+    e2e_t = torch.tensor([e0.elapsed_time(e1) / args.steps], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+
+    # One full pass over the BVSS tiles (5 bytes per slice) plus a label read
+    # and write per vertex: the least traffic of any label propagation.
+    algo = 5 * int(info.no_slices) + 8 * n
+    kern_s = float(np.mean(kern))
+    peak, peak_kind = measured_peak()
+    achieved = algo / kern_s / 1e9
+    result = {
+        "metric": "CC time (BVSS label propagation, labels = component minimum id)",
+        "value": round(ms, 4), "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms, 4), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generator; see config)",
+        "config": {"workload": args.workload, "description": desc, "n": n, "nnz_directed": csc.nnz,
+                   "bvss_slices": int(info.no_slices), "iterations": int(st0.iterations),
+                   "components": int(st0.no_components),
+                   "l2": "inputs larger than L2 (BVSS in HBM), no flush",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "e2e": {"value": round(float(e2e_t.item()), 4), "unit": "ms", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 4 * n},
+        "gpu_launches": 2 * args.steps,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_source": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": algo, "avg_launch_ms": round(kern_s * 1e3, 4)},
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle as O
+        t = time.perf_counter()
+        O.cc_csc(n, csc.col_ptrs, csc.rows)
+        secs = time.perf_counter() - t
+        result["cpu_baseline"] = {"value": round(secs * 1e3, 2), "unit": "ms", "cores": 1, "kind": "port",
+                                  "sample": f"the whole graph once, {secs:.1f} s"}
+    return result
+
+
 def cpu_baseline(csc, csr, sources, deg, args):
     """OpenMP direction-optimising BFS (the oracle's CPU baseline) on the
     host cores, over a bounded sample of the sources (~10-30 s)."""
@@ -618,6 +712,25 @@ def run_reference(args, rank, world):
     n = csc.n
     deg = np.diff(csr.col_ptrs.astype(np.int64))
     ref = O.RefGraph.from_bvss(n, bvss.arrays(), bvss.full_padding, bvss.update_divergence, csr.col_ptrs, csr.rows)
+    if kind == "cc":
+        for _ in range(args.warmup):
+            ref.cc_raw(n)
+        with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+            ts = [ref.cc_raw(n)[1] for _ in range(args.steps)]
+        ms = float(np.mean(ts)) * 1e3
+        return {
+            "impl": "reference", "metric": "CC time (BVSS label propagation, labels = component minimum id)",
+            "value": round(ms, 4), "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms, 4), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32", "data": "synthetic (seeded generator; see config)",
+            "config": {"workload": args.workload, "description": desc, "n": n,
+                       "timing": "reference convention: launch -> cudaDeviceSynchronize around the label "
+                                 "propagation kernels (CC/BVSSCCKernel.cuh), graph upload untimed"},
+            "cpu_baseline": {"value": round(ms, 4), "unit": "ms", "cores": 0, "kind": "reference",
+                             "sample": f"{args.steps} runs on the GPU (the reference's CC kernels built for sm_100a)"},
+            "e2e": {"value": round(ms, 4), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "clocks": clocks.summary(),
+        }
     sample = sources[: args.ref_sources]
     variant = ["BVSSBFS8EnhancedSliceSize8NoMasks4", "FullPad", "LazySwitching", "LazyFullPad"][ref.bfs_variant()]
     mr = {}
@@ -687,6 +800,8 @@ def main():
             res = run_reference(args, rank, world)
         elif WORKLOADS[args.workload][0] == "mbfs":
             res = run_mbfs(args, rank, world)
+        elif WORKLOADS[args.workload][0] == "cc":
+            res = run_cc(args, rank, world)
         elif WORKLOADS[args.workload][0] == "serving":
             res = run_serving(args, rank, world) if rank == 0 else None
         else:

@@ -101,6 +101,46 @@ struct Enqueue {
     uint32_t units;
 };
 
+// Per-block state of the current level, written by thread 0 inside the
+// level barrier: the finished level's counters and where this level's
+// queue entries start (packed entries/units, cumulative).
+struct LevelShared {
+    unsigned long long dq, dd, dg;  // finished level: queue added, discovered, degree sum
+    unsigned long long heavy;       // pull level: packed heavy-list items/chunks still to scan
+    unsigned long long qbase;       // cumulative queue position at the start of this level
+    uint32_t slot;                  // this level's counter slot (level % 3)
+    uint32_t ok;
+};
+__shared__ LevelShared s_lv;
+
+// End-of-level barrier: every block arrives; thread 0 then reads the
+// finished level's counters (slot `done` % 3) into s_lv. If `heavy_check`
+// and the level queued heavy in-neighbour lists, the level is not finished
+// yet: s_lv.heavy says so and the queue base stays, so the heavy phase
+// keeps appending to the same level (a second call then ends it).
+// Otherwise the queue base and slot advance to level done + 1.
+// Returns false if the run has an error recorded.
+__device__ __forceinline__ bool level_barrier(RunCounters* c, uint32_t done, bool heavy_check) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint64_t v = barrier_arrive_wait(c);
+        const unsigned long long* l = c->lvl[done % 3];
+        const uint64_t dq = ld_relaxed64(&l[0]), dd = ld_relaxed64(&l[1]), dg = ld_relaxed64(&l[2]);
+        const uint64_t hv = heavy_check ? ld_relaxed64(&l[3]) : 0;
+        s_lv.heavy = hv;
+        if (hv == 0) {
+            s_lv.dq = dq;
+            s_lv.dd = dd;
+            s_lv.dg = dg;
+            s_lv.qbase += dq;  // fields cannot carry: entries < 2^28, units < 2^36
+            s_lv.slot = (done + 1) % 3;
+        }
+        s_lv.ok = (v & kArriveError) == 0;
+    }
+    __syncthreads();
+    return s_lv.ok;
+}
+
 template <bool ALIGNED>
 __device__ __forceinline__ void flush_enqueue(const BfsArgs& a, Enqueue& q, int limit = -1) {
     const uint32_t lane = threadIdx.x & 31;
@@ -108,7 +148,7 @@ __device__ __forceinline__ void flush_enqueue(const BfsArgs& a, Enqueue& q, int 
     const uint64_t mine = ((uint64_t)q.cnt << kQShift) | q.units;
     const uint64_t incl = warp_inclusive_scan64(mine);
     uint64_t base = 0;
-    if (lane == 31) base = atomicAdd((unsigned long long*)&a.ctr->queue, (unsigned long long)incl);
+    if (lane == 31) base = atomicAdd(&a.ctr->lvl[s_lv.slot][0], (unsigned long long)incl) + s_lv.qbase;
     base = __shfl_sync(0xFFFFFFFFu, base, 31);
     const uint64_t excl = base + incl - mine;
     uint32_t e = (uint32_t)(excl >> kQShift);
@@ -299,14 +339,24 @@ __device__ __forceinline__ void bfs_prologue(const BfsArgs& a, uint32_t tid, uin
             a.q_off[0] = 0;
             q = (1ull << kQShift) | units;
         }
-        const uint64_t deg = a.g.csr_ptrs[src + 1] - a.g.csr_ptrs[src];
-        c->queue = q;
-        c->discovered = 1;
-        c->degree = deg;
-        c->snap_queue[0] = q;
-        c->snap_discovered[0] = 1;
-        c->snap_degree[0] = deg;
+        // level 0 = the source (slot 0); slots 1 and 2 start zeroed
+        c->lvl[0][0] = q;
+        c->lvl[0][1] = 1;
+        c->lvl[0][2] = a.g.csr_ptrs[src + 1] - a.g.csr_ptrs[src];
     }
+    if (threadIdx.x == 0) s_lv.qbase = 0;
+}
+
+// Add a warp's discoveries (count, degree sum) to a level's counters and
+// reset the per-thread sums.
+__device__ __forceinline__ void add_level_counts(unsigned long long* lvl, uint32_t& disc, uint64_t& deg) {
+    const uint64_t wd = warp_sum64(disc), wg = warp_sum64(deg);
+    if ((threadIdx.x & 31) == 0 && wd) {
+        atomicAdd(&lvl[1], (unsigned long long)wd);
+        atomicAdd(&lvl[2], (unsigned long long)wg);
+    }
+    disc = 0;
+    deg = 0;
 }
 
 template <bool ALIGNED, bool MMA, bool PARENTS>
@@ -320,20 +370,28 @@ __global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(BfsArgs a) {
     RunCounters* c = a.ctr;
 
     bfs_prologue<ALIGNED>(a, tid, nth);
-    if (!grid_barrier(c, 1)) return;
+    if (!level_barrier(c, 0, false)) return;
 
     // Cumulative counters at the end of levels L-3 and L-2.
     uint32_t E3 = 0, E2 = 0, U2 = 0;
     uint64_t D2 = 0, G2 = 0;
+    uint64_t nf_prev = 0;  // vertices discovered at level L-2
     int dir = a.direction == BLEST_DIR_PULL ? BLEST_DIR_PULL : BLEST_DIR_PUSH;
 
     for (uint32_t level = 1;; ++level) {
-        const uint32_t par = (level - 1) & 1;
-        const uint64_t q1 = c->snap_queue[par];
-        const uint32_t E1 = (uint32_t)(q1 >> kQShift), U1 = (uint32_t)(q1 & kQUnitMask);
-        const uint64_t D1 = c->snap_discovered[par], G1 = c->snap_degree[par];
+        // cumulative counters at the end of level L-1
+        const uint32_t E1 = E2 + (uint32_t)(s_lv.dq >> kQShift), U1 = U2 + (uint32_t)(s_lv.dq & kQUnitMask);
+        const uint64_t D1 = D2 + s_lv.dd, G1 = G2 + s_lv.dg;
         const uint64_t nf = D1 - D2;  // discovered at level L-1
-        if (nf == 0) {
+        if (nf == 0 || level > g.n + 1) {
+            if (tid == 0) {
+                c->discovered = D1;
+                c->degree = G1;
+            }
+            if (nf != 0) {
+                set_error(c, BLEST_ERR_LEVEL_CAP);
+                break;
+            }
             if (tid == 0) {
                 c->levels = level - 1;  // max level + 1
                 if (a.trace && level <= BLEST_TRACE_CAPACITY) {
@@ -347,19 +405,19 @@ __global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(BfsArgs a) {
             }
             break;
         }
-        if (level > g.n + 1) {
-            set_error(c, BLEST_ERR_LEVEL_CAP);
-            break;
-        }
         if (a.direction == BLEST_DIR_AUTO) {
             // Beamer's switch in edge/vertex units: to pull when the new
             // frontier's edges m_f exceed the unvisited edges m_u / alpha,
             // back to push when the new frontier has fewer than n / beta
-            // vertices.
+            // vertices. As in Beamer's heuristic, only a growing frontier
+            // starts a pull phase: late levels have tiny m_u, and a pull
+            // level there would scan every vertex word for a few vertices.
             const double mf = (double)(G1 - G2), mu = (double)(g.degree_total - G1);
-            if (dir == BLEST_DIR_PUSH && mf * a.alpha > mu) dir = BLEST_DIR_PULL;
+            const bool growing = nf > nf_prev;
+            if (dir == BLEST_DIR_PUSH && mf * a.alpha > mu && growing) dir = BLEST_DIR_PULL;
             else if (dir == BLEST_DIR_PULL && (double)nf * a.beta < (double)g.n) dir = BLEST_DIR_PUSH;
         }
+        nf_prev = nf;
         if (a.trace && tid == 0 && level <= BLEST_TRACE_CAPACITY) {
             blest_level_trace& t = a.trace[level - 1];
             t.start_ns = global_ns();
@@ -372,13 +430,22 @@ __global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(BfsArgs a) {
             if (level >= 2) a.trace[level - 2].longest_scan = ld_relaxed64(&c->aux[6 + ((level - 1) & 1)]);
             c->aux[6 + ((level - 1) & 1)] = 0;
         }
-        // heavy-list counter of the next level (its slot was last used at level-1)
-        if (tid == 0) c->aux[2 + ((level + 1) & 1)] = 0;
+        // counters of level L+1 (their slot was last read at the end of L-2)
+        if (tid < 4) c->lvl[(level + 1) % 3][tid] = 0;
         uint32_t* fprev = frontier_buf(a, level - 1);
         uint32_t* fcur = frontier_buf(a, level);
         uint8_t* fclr = reinterpret_cast<uint8_t*>(frontier_buf(a, level + 1));
         uint32_t* fsum = summary_buf(a, level);
         uint32_t* sclr = summary_buf(a, level + 1);
+
+        // Pull levels: frontier test of an in-neighbour through the level's
+        // summary (staged in shared memory) and then its frontier word.
+        extern __shared__ uint32_t s_sum[];
+        auto in_frontier = [&](uint32_t v) -> bool {
+            const uint32_t sb = (v >> 5) >> a.sum_shift;
+            if (!((s_sum[sb >> 5] >> (sb & 31)) & 1u)) return false;
+            return (__ldcg(&fprev[v >> 5]) >> (v & 31)) & 1u;
+        };
 
         Enqueue q;
         q.cnt = 0;
@@ -430,15 +497,9 @@ __global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(BfsArgs a) {
             // frontier neighbour. A neighbour's frontier word is read from L2
             // only when the level's summary (staged in shared memory) says
             // it is non-empty; vertices without in-neighbours are skipped.
-            extern __shared__ uint32_t s_sum[];
             const uint32_t* sprev = summary_buf(a, level - 1);
             for (uint32_t i = threadIdx.x; i < a.sum_words; i += blockDim.x) s_sum[i] = __ldcg(&sprev[i]);
             __syncthreads();
-            auto in_frontier = [&](uint32_t v) -> bool {
-                const uint32_t sb = (v >> 5) >> a.sum_shift;
-                if (!((s_sum[sb >> 5] >> (sb & 31)) & 1u)) return false;
-                return (__ldcg(&fprev[v >> 5]) >> (v & 31)) & 1u;
-            };
             const uint32_t W = (g.n + 31) / 32;
             const uint32_t tailMask = (g.n & 31) ? ((1u << (g.n & 31)) - 1) : 0xFFFFFFFFu;
             uint32_t longest = 0;
@@ -486,12 +547,12 @@ __global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(BfsArgs a) {
                     }
                 }
                 // Very long lists go to the heavy queue (all warps split them
-                // after the mid-level barrier).
+                // after the level barrier).
                 {
                     const bool heavy = !found && p < pe && pe - p > a.heavy_min;
                     if (heavy) {
                         const uint32_t chunks = (pe - p + kHeavyChunk - 1) / kHeavyChunk;
-                        const uint64_t slot = atomicAdd(&c->aux[2 + (level & 1)],
+                        const uint64_t slot = atomicAdd(&c->lvl[level % 3][3],
                                                         (unsigned long long)((1ull << kQShift) | chunks));
                         const uint32_t idx = (uint32_t)(slot >> kQShift);
                         if (idx < a.heavy_cap) {
@@ -553,9 +614,26 @@ __global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(BfsArgs a) {
             }
             if (a.trace && lane == 0 && longest) atomicMax(&c->aux[6 + (level & 1)], (unsigned long long)longest);
             flush_enqueue<ALIGNED>(a, q);
-            // Heavy lists: every warp takes an equal share of the pieces.
-            if (!grid_barrier(c, level & 1)) return;
-            const uint64_t hq = ld_relaxed64(&c->aux[2 + (level & 1)]);
+        }
+
+        flush_enqueue<ALIGNED>(a, q);  // whatever is still buffered
+        // Clear the frontier bytes written two levels back (queue of L-2).
+        for (uint32_t e = E3 + tid; e < E2; e += nth) {
+            const uint32_t r = __ldcg(&a.q_rset[e]);
+            fclr[r] = 0;
+            sclr[((r >> 2) >> a.sum_shift) >> 5] = 0u;
+        }
+
+        add_level_counts(c->lvl[level % 3], disc, deg);
+        if (tid == 0) {
+            if (dir == BLEST_DIR_PUSH) c->push_levels++;
+            else c->pull_levels++;
+        }
+        if (!level_barrier(c, level, dir == BLEST_DIR_PULL)) return;
+        if (s_lv.heavy) {
+            // Heavy lists of this pull level: every warp takes an equal
+            // share of the pieces, then the level ends with a second barrier.
+            const uint64_t hq = s_lv.heavy;
             const uint32_t hitems = min((uint32_t)(hq >> kQShift), a.heavy_cap);
             const uint32_t hchunks = (uint32_t)(hq & kQUnitMask);
             if (hitems) {
@@ -603,26 +681,10 @@ __global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(BfsArgs a) {
                     flush_enqueue<ALIGNED>(a, q, kEnqueueCap - 1);
                 }
             }
+            flush_enqueue<ALIGNED>(a, q);
+            add_level_counts(c->lvl[level % 3], disc, deg);
+            if (!level_barrier(c, level, false)) return;
         }
-
-        flush_enqueue<ALIGNED>(a, q);  // whatever is still buffered
-        // Clear the frontier bytes written two levels back (queue of L-2).
-        for (uint32_t e = E3 + tid; e < E2; e += nth) {
-            const uint32_t r = __ldcg(&a.q_rset[e]);
-            fclr[r] = 0;
-            sclr[((r >> 2) >> a.sum_shift) >> 5] = 0u;
-        }
-
-        const uint64_t wd = warp_sum64(disc), wg = warp_sum64(deg);
-        if (lane == 0 && wd) {
-            atomicAdd((unsigned long long*)&c->discovered, (unsigned long long)wd);
-            atomicAdd((unsigned long long*)&c->degree, (unsigned long long)wg);
-        }
-        if (tid == 0) {
-            if (dir == BLEST_DIR_PUSH) c->push_levels++;
-            else c->pull_levels++;
-        }
-        if (!grid_barrier(c, level & 1)) return;
         E3 = E2;
         E2 = E1;
         U2 = U1;

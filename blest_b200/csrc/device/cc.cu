@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(512) cc_persistent_kernel(CcArgs a) {
         }
         const uint32_t wc = (uint32_t)warp_sum64(changes);
         if (lane == 0 && wc) atomicAdd(&a.qctr[4], (unsigned long long)wc);
-        if (!grid_barrier(c, it & 1)) return;
+        if (!grid_barrier(c)) return;
     }
 }
 

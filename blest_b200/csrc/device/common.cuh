@@ -41,36 +41,31 @@ struct DevGraph {
     const uint32_t* has_in;     // ceil(n/32) words: bit v = v has an in-neighbour (may be null)
 };
 
-// Grid barrier geometry: blocks arrive in groups of kBarrierGroup on
-// separate counters; the last block of each group arrives at the root.
-constexpr uint32_t kBarrierGroup = 16;
-constexpr uint32_t kBarrierMaxGroups = 64;
+// Bit 63 of the barrier's arrival counter: some block recorded an error.
+constexpr unsigned long long kArriveError = 1ull << 63;
 
-// Counters of one BFS/CC run (zeroed before every run).
+// Counters of one BFS/CC/MBFS run (zeroed before every run).
 struct RunCounters {
-    unsigned long long queue;       // packed entries/units, cumulative
-    unsigned long long discovered;  // vertices discovered, cumulative
-    unsigned long long degree;      // degree sum of discovered vertices
-    unsigned long long grab[2];     // dynamic work counters, by level parity
-    unsigned int bar_count;
-    unsigned int bar_gen;
+    unsigned long long discovered;  // BFS: vertices reached (written at exit); CC: components
+    unsigned long long degree;      // BFS: degree sum of the reached vertices (written at exit)
     unsigned int error;
     unsigned int levels;            // last level with discoveries
     unsigned int push_levels;
     unsigned int pull_levels;
     unsigned int iterations;
-    unsigned int pad;
-    // Snapshot taken by the last block to reach a barrier, by parity.
-    unsigned long long snap_queue[2];
-    unsigned long long snap_discovered[2];
-    unsigned long long snap_degree[2];
-    unsigned int snap_flag[2];
-    unsigned int pad2[2];
-    // CC: packed queue counters of 4 iteration slots + cumulative label updates.
+    unsigned int pad[7];
+    // Slots reused across levels/iterations (queue counters, heavy-list
+    // counters, trace maxima); each kernel documents its own use.
     unsigned long long aux[8];
-    // Hierarchical grid barrier: one arrival counter per group of
-    // kBarrierGroup blocks, each on its own 128-byte line, plus the root.
-    unsigned int bar_group[kBarrierMaxGroups * 32];
+    // BFS per-level counters, slot = level % 3: packed queue entries/units
+    // added during the level, vertices discovered, their degree sum.
+    // Counters of level L are read after the barrier that ends L and
+    // zeroed during level L + 2, so no block ever needs a snapshot.
+    unsigned long long lvl[3][4];
+    // Grid barrier: monotone arrival count (bits 0-62) + error flag (bit 63),
+    // alone on its 128-byte line.
+    alignas(128) unsigned long long arrive;
+    unsigned long long pad_arrive[15];
 };
 
 __device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
@@ -101,54 +96,56 @@ __device__ __forceinline__ uint64_t global_ns() {
 __device__ __forceinline__ uint4 ld_stream(const uint4* p) { return __ldcs(p); }
 __device__ __forceinline__ uint32_t ld_stream(const uint32_t* p) { return __ldcs(p); }
 
-__device__ __forceinline__ void set_error(RunCounters* c, uint32_t code) { atomicCAS(&c->error, 0u, code); }
+__device__ __forceinline__ uint64_t ld_acquire64(const unsigned long long* p) {
+    uint64_t v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
 
-// Grid-wide barrier for a cooperative (co-resident) launch, with a bounded
-// wait: a block that waits longer than kBarrierTimeoutNs records
-// BLEST_ERR_BARRIER_TIMEOUT and leaves; every caller then sees the error and
-// returns, so no wait is unbounded. Arrival is two-level (a counter per
-// group of kBarrierGroup blocks, then the root) so that no single address
-// takes more than ~max(kBarrierGroup, groups) atomics. Before releasing the
-// other blocks, the last arriving block copies the run counters into the
-// snapshot slot of this barrier's parity, so all blocks read identical
-// values afterwards even while others already update the live counters.
-// Returns false if the run has an error recorded.
-__device__ __forceinline__ bool grid_barrier(RunCounters* c, uint32_t parity) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const uint32_t gen = ld_acquire(&c->bar_gen);
-        __threadfence();
-        const uint32_t grp = blockIdx.x / kBarrierGroup;
-        const uint32_t groups = (gridDim.x + kBarrierGroup - 1) / kBarrierGroup;
-        const uint32_t gsize = min(kBarrierGroup, gridDim.x - grp * kBarrierGroup);
-        bool root = false;
-        if (atomicAdd(&c->bar_group[grp * 32], 1u) == gsize - 1) {
-            c->bar_group[grp * 32] = 0;  // nobody touches it again before the release
-            __threadfence();
-            root = atomicAdd(&c->bar_count, 1u) == groups - 1;
-        }
-        if (root) {
-            c->snap_queue[parity] = ld_relaxed64(&c->queue);
-            c->snap_discovered[parity] = ld_relaxed64(&c->discovered);
-            c->snap_degree[parity] = ld_relaxed64(&c->degree);
-            c->bar_count = 0;
-            __threadfence();
-            st_release(&c->bar_gen, gen + 1);
-        } else {
-            const uint64_t t0 = global_ns();
-            uint32_t spins = 0;
-            while (ld_acquire(&c->bar_gen) == gen) {
-                if ((++spins & 63) == 0 && global_ns() - t0 > kBarrierTimeoutNs) {
-                    set_error(c, BLEST_ERR_BARRIER_TIMEOUT);
-                    break;
-                }
-                if (spins > 64) __nanosleep(32);
+// Record the first error of the run and flag it in the barrier word, so
+// the next barrier reports it to every block without an extra load.
+__device__ __forceinline__ void set_error(RunCounters* c, uint32_t code) {
+    atomicCAS(&c->error, 0u, code);
+    atomicOr(&c->arrive, kArriveError);
+}
+
+// Thread 0's half of the grid barrier: arrive and wait. The arrival count
+// only grows (one per block per barrier), so the k-th barrier is complete
+// when it reaches k * gridDim.x; the value the atomic returns says which k
+// this block is at, so no generation word has to be read or reset, and the
+// last block to arrive leaves at once. The wait is bounded: a block that
+// waits longer than kBarrierTimeoutNs records BLEST_ERR_BARRIER_TIMEOUT and
+// leaves. Returns the final counter value (bit 63 = error recorded).
+__device__ __forceinline__ uint64_t barrier_arrive_wait(RunCounters* c) {
+    __threadfence();
+    const uint64_t n = gridDim.x;
+    uint64_t v = atomicAdd(&c->arrive, 1ull);
+    const uint64_t target = ((v & ~kArriveError) / n + 1) * n;
+    ++v;
+    if ((v & ~kArriveError) < target) {
+        const uint64_t t0 = global_ns();
+        uint32_t spins = 0;
+        while (((v = ld_acquire64(&c->arrive)) & ~kArriveError) < target) {
+            if ((++spins & 31) == 0 && global_ns() - t0 > kBarrierTimeoutNs) {
+                set_error(c, BLEST_ERR_BARRIER_TIMEOUT);
+                return kArriveError;
             }
-            __threadfence();
+            if (spins > 256) __nanosleep(20);
         }
     }
+    __threadfence();
+    return v;
+}
+
+// Grid-wide barrier for a cooperative (co-resident) launch. Returns false
+// if the run has an error recorded (every caller then returns), so no wait
+// is unbounded.
+__device__ __forceinline__ bool grid_barrier(RunCounters* c) {
+    __shared__ uint32_t s_ok;
     __syncthreads();
-    return ld_relaxed(&c->error) == 0;
+    if (threadIdx.x == 0) s_ok = (barrier_arrive_wait(c) & kArriveError) == 0;
+    __syncthreads();
+    return s_ok;
 }
 
 // Warp-inclusive scan of a 64-bit value.

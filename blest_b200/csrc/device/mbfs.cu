@@ -91,8 +91,7 @@ __global__ void __launch_bounds__(512, 2) mbfs_persistent_kernel(MbfsArgs a) {
     RunCounters* c = a.ctr;
     const uint32_t n = g.n;
     const uint32_t Wn = (n + 31) / 32;
-    uint32_t parity = 0;
-    auto barrier = [&]() -> bool { return grid_barrier(c, (parity++) & 1); };
+    auto barrier = [&]() -> bool { return grid_barrier(c); };
 
     const uint32_t groups = (a.k + a.group_width - 1) / a.group_width;
     for (uint32_t grp = 0; grp < groups; ++grp) {
