@@ -51,6 +51,11 @@ WORKLOADS = {
     "mbfs_rmat22": ("mbfs", ("rmat", 22, 16), "jaccard", 65536, 1024,
                     "multi-source BFS, RMAT scale 22 ef 16, Jaccard window 65536, 1024 seeded sources "
                     "in bit-packed groups of 128"),
+    "mbfs_multi256": ("mbfs_multi", None, "jaccard", 65536, 8,
+                      "256 independent RMAT graphs (a,b,c)=(.57,.19,.19), n = round(2^clip(N(14, 2.43), 10, 18)) "
+                      "(RMAT on 2^ceil(log2 n) vertices, seeded permutation, induced on ids < n), edge factor "
+                      "uniform 4..32, Jaccard window 65536, 8 seeded sources each; one multi-graph MBFS launch "
+                      "replayed from a captured CUDA graph"),
 }
 
 SEED = 1
@@ -307,6 +312,263 @@ def run_mbfs(args, rank, world):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_source": peak_kind, "traffic": None,
                      "algorithmic_bytes_per_launch": out_bytes, "note": "output levels only (lower bound)"},
+        "clocks": clocks.summary(),
+    }
+
+
+MULTI_GRAPHS = 256
+MULTI_SOURCES = 8
+MULTI_SIGMA = 4.0 / 1.6449  # log2-space sigma: 5th..95th percentile of N(14, sigma) = 10..18
+
+
+def multi_graph_specs(count: int = MULTI_GRAPHS):
+    """(n, edge factor) of the batch: n = round(2^clip(N(14, sigma), 10, 18)),
+    edge factor uniform in 4..32, from the recorded seed."""
+    rng = np.random.default_rng(SEED)
+    exps = np.clip(rng.normal(14.0, MULTI_SIGMA, count), 10.0, 18.0)
+    ns = np.round(2.0 ** exps).astype(np.int64)
+    efs = rng.integers(4, 33, count)
+    return [(int(n), int(ef)) for n, ef in zip(ns, efs)]
+
+
+def rmat_n(n: int, ef: int, seed: int):
+    """RMAT graph on exactly n vertices: the subgraph induced by ids [0, n)
+    of a seeded-permuted RMAT graph of 2^ceil(log2 n) vertices whose edge
+    factor is raised by 2^s / n, so that about n * ef edges survive."""
+    from blest_b200 import Csc
+    s = max(1, int(np.ceil(np.log2(n))))
+    ef2 = max(1, int(round(ef * (1 << s) / n)))
+    big = Csc.rmat(s, ef2, 0.57, 0.19, 0.19, seed=seed, permute_seed=seed)
+    if big.n == n:
+        return big
+    cp = big.col_ptrs.astype(np.int64)
+    rows = big.rows
+    col = np.repeat(np.arange(big.n, dtype=np.int64), np.diff(cp))
+    keep = (col < n) & (rows < n)
+    ncp = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(np.bincount(col[keep], minlength=n)[:n], out=ncp[1:])
+    return Csc.from_arrays(n, ncp.astype(np.uint32), np.ascontiguousarray(rows[keep], dtype=np.uint32))
+
+
+def _multi_worker_init():
+    os.environ["OMP_NUM_THREADS"] = "2"
+
+
+def _build_multi_graph(job):
+    """One graph of the batch: generate, sample k sources (original ids),
+    Jaccard-reorder, build the BVSS, save both; returns the sources in
+    reordered ids."""
+    from blest_b200 import Bvss
+    i, n, ef, k, tag = job
+    csc = rmat_n(n, ef, SEED + 1 + i)
+    s = csc.sample_sources(k, SEED + i)
+    inv = csc.reorder("jaccard", window=65536)
+    csc.save_bin(f"{tag}/g{i}_csc.bin")
+    Bvss.build(csc).save_bin(f"{tag}/g{i}_bvss.bin")
+    return i, np.asarray(inv[s], dtype=np.uint32)
+
+
+def prepare_multi(cache_dir: Path, rank: int, count: int = MULTI_GRAPHS, k: int = MULTI_SOURCES):
+    """The batch's graphs (Jaccard-reordered CSC + BVSS) and k sources each,
+    built by rank 0 into the cache and loaded by every rank."""
+    from blest_b200 import Bvss, Csc
+    tag = cache_dir / f"mbfs_multi{count}"
+    done = tag / "ready"
+    if rank == 0 and not done.exists():
+        import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
+        tag.mkdir(parents=True, exist_ok=True)
+        t0 = time.time()
+        specs = multi_graph_specs(count)
+        jobs = [(i, n, ef, k, str(tag)) for i, (n, ef) in sorted(enumerate(specs), key=lambda x: -x[1][0] * x[1][1])]
+        workers = max(1, min(16, (os.cpu_count() or 2) // 2))
+        # spawn: the parent already holds a CUDA context
+        with ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn"), initializer=_multi_worker_init) as ex:
+            res = dict(ex.map(_build_multi_graph, jobs))
+        np.save(str(tag / "sources.npy"), np.stack([res[i] for i in range(count)]).astype(np.uint32))
+        done.write_text("ok")
+        log(f"[prep] mbfs_multi{count}: {time.time() - t0:.1f}s on {workers} processes")
+    else:
+        deadline = time.time() + 3600
+        while not done.exists():
+            if time.time() > deadline:
+                raise TimeoutError("graph cache not ready")
+            time.sleep(1.0)
+    graphs = []
+    for i in range(count):
+        csc = Csc.load_bin(str(tag / f"g{i}_csc.bin"))
+        graphs.append((csc, Bvss.load_bin(str(tag / f"g{i}_bvss.bin"))))
+    return graphs, np.load(str(tag / "sources.npy"))
+
+
+def run_mbfs_multi(args, rank, world):
+    """Many graphs in one persistent launch: 256 RMAT graphs of lognormal
+    size, 8 sources each, run as one multi-graph MBFS plan replayed from a
+    captured CUDA graph; next to the same (graph, source) pairs run one
+    single-source BFS launch each, and one MBFS launch per graph."""
+    import torch
+    import torch.distributed as dist
+    import blest_b200
+    from blest_b200 import Graph, MbfsPlan, Workspace
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    blest_b200.init(dev)
+    kind, gen, order, window, nsrc, desc = WORKLOADS[args.workload]
+    t0 = time.time()
+    hosts, sources = prepare_multi(Path(args.cache), rank, MULTI_GRAPHS, nsrc)
+    t_prep = time.time() - t0
+    graphs = [Graph(b, c) for c, b in hosts]
+    ns = [c.n for c, _ in hosts]
+    k = sources.shape[1]
+    total = sum(ns) * k
+    out = torch.empty(total, dtype=torch.int32, device="cuda")
+    views, o = [], 0
+    for n in ns:
+        views.append(out[o:o + k * n].view(k, n))
+        o += k * n
+    barrier = (lambda: dist.barrier()) if world > 1 else (lambda: None)
+
+    def make(p):
+        return MbfsPlan([(g, sources[i], views[i].data_ptr()) for i, g in enumerate(graphs)], **p)
+
+    # autotune: CTAs per SM and the pull threshold (8 sources fill one
+    # 32-wide group)
+    table = []
+    best = None
+    for bps in (1, 2):
+        for pf in (1 / 16, 1 / 64, 1 / 256):
+            p = {"group_width": 32, "blocks_per_sm": bps, "pull_fraction": pf}
+            plan = make(p)
+            plan.run()
+            t = min(plan.run().time for _ in range(3))
+            table.append((t, p))
+            if best is None or t < best[0]:
+                best = (t, p)
+            plan.close()
+    tuned = best[1]
+    log(f"[autotune] multi-graph plan best {tuned}: {best[0] * 1e3:.3f} ms (worst {max(table, key=lambda r: r[0])[0] * 1e3:.3f})")
+    plan = make(tuned)
+    info = plan.info()
+    plan.run()
+    # reached edges and algorithmic bytes per step, from the levels
+    mr, s_r, v_r, n_r = 0, 0, 0, 0
+    for (csc, bvss), lv in zip(hosts, views):
+        deg = torch.from_numpy(np.diff(csc.col_ptrs.astype(np.int64))).cuda()
+        reached = lv != -1
+        mr += int(((reached.to(torch.int64) * deg).sum(1) // 2).sum().item())
+        n_r += int(reached.sum().item())
+        anyr = reached.any(0).cpu().numpy()
+        rsets = np.unique(np.nonzero(anyr)[0] >> 3)
+        a = bvss.arrays()
+        rp, ssp = a["real_ptrs"], a["slice_set_ptrs"]
+        v_r += int((rp[rsets + 1].astype(np.int64) - rp[rsets]).sum())
+        s_r += int((ssp[rp[rsets + 1]].astype(np.int64) - ssp[rp[rsets]].astype(np.int64)).sum())
+    algo = 5 * s_r + 12 * v_r + 4 * n_r
+    if rank == 0 and not args.skip_check:
+        import oracle as O
+        big = int(np.argmax(ns))
+        for i in (0, 1, big, len(graphs) - 1):
+            csc = hosts[i][0]
+            for j in (0, k - 1):
+                want = O.bfs_csc(csc.n, csc.col_ptrs, csc.rows, int(sources[i][j]))
+                if not np.array_equal(views[i][j].cpu().numpy().view(np.uint32), want):
+                    raise SystemExit(f"multi-graph MBFS levels differ from the oracle (graph {i}, source {j})")
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        plan.run()
+    barrier()
+    torch.cuda.synchronize()
+    kern = []
+    with ClockSampler(dev) as clocks:
+        t_start = time.perf_counter()
+        for _ in range(args.steps):
+            plan.launch()
+            kern.append(plan.sync().time)
+        wall = time.perf_counter() - t_start
+    barrier()
+    ms_t = torch.tensor([sum(kern) * 1e3], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms = float(ms_t.item())
+    value = mr * args.steps * world / (ms * 1e-3) / 1e9
+
+    # plain: one single-source BFS launch per (graph, source)
+    wss = [Workspace(g) for g in graphs]
+    st = torch.cuda.Stream()
+    scratch = torch.empty(max(ns), dtype=torch.int32, device="cuda")
+    for i in range(min(4, len(graphs))):
+        wss[i].bfs_async(int(sources[i][0]), scratch.data_ptr(), st.cuda_stream)
+    st.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for i, w in enumerate(wss):
+        for j in range(k):
+            w.bfs_async(int(sources[i][j]), scratch.data_ptr(), st.cuda_stream)
+    e1.record(st)
+    st.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+    plain = mr / (plain_ms * 1e-3) / 1e9
+    for w in wss:
+        w.close()
+    # one MBFS launch per graph (blest_mbfs_ws on each graph in turn)
+    from blest_b200 import _lib as L
+    import ctypes as C
+    pm = L.MbfsParams(32, tuned["blocks_per_sm"], 0, tuned["pull_fraction"])
+    stt = L.MbfsStats()
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    for i, g in enumerate(graphs):
+        src = np.ascontiguousarray(sources[i], dtype=np.uint32)
+        L.call("blest_mbfs", g._h, src.ctypes.data_as(L.P(L.u32)), k, views[i].data_ptr(), L.MEM_DEVICE,
+               C.byref(pm), C.byref(stt))
+    per_graph_s = time.perf_counter() - t1
+    per_graph = mr / per_graph_s / 1e9
+
+    # e2e: new sources (H2D) each step, replay, all levels to pinned host memory
+    pinned = torch.empty(total, dtype=torch.int32, pin_memory=True)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        for i in range(len(graphs)):
+            plan.set_sources(i, sources[i])
+        plan.launch()
+        plan.sync()
+        pinned.copy_(out, non_blocking=True)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = ev0.elapsed_time(ev1)
+    e2e = mr * args.steps / (e2e_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peak()
+    kern_s = float(np.mean(kern))
+    achieved = algo / kern_s / 1e9
+    plan.close()
+    return {
+        "metric": "batched MBFS GTEPS, many graphs in one launch (sum over (graph, source) of reached edges / batch time)",
+        "value": round(value, 3), "unit": "GTEPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generator; see config)",
+        "config": {"workload": args.workload, "description": desc, "graphs": len(graphs),
+                   "sources_per_graph": k, "vertices_total": int(sum(ns)),
+                   "n_min": int(min(ns)), "n_median": int(np.median(ns)), "n_max": int(max(ns)),
+                   "nnz_total": int(sum(c.nnz for c, _ in hosts)), "joined_n": int(info.n),
+                   "captured_cuda_graph": bool(info.captured), "grid_blocks": int(info.grid_blocks),
+                   "autotuned": tuned, "autotune_table_ms": [[round(t * 1e3, 3), p] for t, p in table],
+                   "reached_edges_per_step": mr,
+                   "plain_one_launch_per_source_gteps": round(plain, 3),
+                   "speedup_vs_plain": round(value / world / plain, 2),
+                   "one_mbfs_launch_per_graph_gteps": round(per_graph, 3),
+                   "speedup_vs_per_graph": round(value / world / per_graph, 2),
+                   "host_wall_ms_per_step": round(wall * 1e3 / args.steps, 4),
+                   "prep_seconds": round(t_prep, 1),
+                   "l2": "outputs larger than L2, no flush"},
+        "e2e": {"value": round(e2e, 3), "unit": "GTEPS", "h2d_bytes_per_step": 4 * int(sources.size),
+                "d2h_bytes_per_step": 4 * total},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_source": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": algo, "avg_launch_ms": round(kern_s * 1e3, 4)},
         "clocks": clocks.summary(),
     }
 
@@ -800,6 +1062,8 @@ def main():
             res = run_reference(args, rank, world)
         elif WORKLOADS[args.workload][0] == "mbfs":
             res = run_mbfs(args, rank, world)
+        elif WORKLOADS[args.workload][0] == "mbfs_multi":
+            res = run_mbfs_multi(args, rank, world)
         elif WORKLOADS[args.workload][0] == "cc":
             res = run_cc(args, rank, world)
         elif WORKLOADS[args.workload][0] == "serving":

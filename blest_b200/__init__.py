@@ -10,7 +10,9 @@ Layers:
   - blest_b200.server: continuous-batching query server.
 """
 from ._lib import BlestError, lib  # noqa: F401  (raises ImportError if the .so is missing)
-from .graph import Bvss, Csc, Graph, Workspace, bfs_params, init, load_ordering, relabel_dense, save_ordering  # noqa: F401,E501
+from .graph import (Bvss, Csc, Graph, MbfsPlan, Workspace, bfs_params, init, load_ordering, mbfs_batch,  # noqa: F401
+                    relabel_dense, save_ordering)
 
-__all__ = ["BlestError", "Bvss", "Csc", "Graph", "Workspace", "bfs_params", "init", "load_ordering", "relabel_dense",
+__all__ = ["BlestError", "Bvss", "Csc", "Graph", "MbfsPlan", "Workspace", "bfs_params", "init", "load_ordering",
+           "mbfs_batch", "relabel_dense",
            "save_ordering", "lib"]

@@ -104,7 +104,7 @@ class DeviceGraphView(C.Structure):
 
 
 class MbfsParams(C.Structure):
-    _fields_ = [("group_width", u32), ("blocks_per_sm", i32), ("threads_per_block", i32)]
+    _fields_ = [("group_width", u32), ("blocks_per_sm", i32), ("threads_per_block", i32), ("pull_fraction", f64)]
 
 
 class MbfsStats(C.Structure):
@@ -129,6 +129,11 @@ class ServerStats(C.Structure):
 
 class MbfsItem(C.Structure):
     _fields_ = [("graph", vp), ("sources", P(u32)), ("k", u32), ("levels_out", vp)]
+
+
+class MbfsPlanInfo(C.Structure):
+    _fields_ = [("items", u32), ("n", u32), ("nnz", u64), ("no_slices", u64), ("groups", u32),
+                ("group_width", u32), ("grid_blocks", i32), ("captured", i32), ("device_bytes", u64)]
 
 
 def _sig(name, args, res=i32):
@@ -187,6 +192,13 @@ _SIGS = {
     "blest_mbfs": [vp, P(u32), u32, vp, i32, P(MbfsParams), P(MbfsStats)],
     "blest_mbfs_batch": [P(MbfsItem), u32, i32, P(MbfsParams), vp, P(MbfsStats)],
     "blest_mbfs_ws": [vp, P(u32), u32, vp, i32, P(MbfsParams), vp, P(MbfsStats)],
+    "blest_mbfs_plan_create": [P(MbfsItem), u32, P(MbfsParams), vp, P(vp)],
+    "blest_mbfs_plan_set_sources": [vp, u32, P(u32)],
+    "blest_mbfs_plan_run": [vp, P(MbfsStats)],
+    "blest_mbfs_plan_launch": [vp],
+    "blest_mbfs_plan_sync": [vp, P(MbfsStats)],
+    "blest_mbfs_plan_info_get": [vp, P(MbfsPlanInfo)],
+    "blest_mbfs_plan_destroy": [vp],
     "blest_workspace_set_grid": [vp, u32],
     "blest_server_create": [P(ServerParams), P(vp)],
     "blest_server_add_graph": [vp, vp, P(u32)],

@@ -34,6 +34,17 @@
 namespace blest {
 namespace dev {
 
+// One graph of a (possibly multi-graph) run: its vertices are
+// [off, off + n) of the resident graph, its k sources start at
+// sources[src_base] (local ids), its levels go to levels[s * n + v].
+struct MbfsPart {
+    uint32_t off;
+    uint32_t n;
+    uint32_t k;
+    uint32_t src_base;
+    uint32_t* levels;
+};
+
 struct MbfsArgs {
     DevGraph g;
     uint32_t* visited;   // n * WORDS
@@ -43,12 +54,49 @@ struct MbfsArgs {
     uint32_t* q_off;
     uint32_t qreg;
     RunCounters* ctr;
-    uint32_t* levels;          // output, source-major: levels[(s) * n + v]
-    const uint32_t* sources;   // all k sources (device)
-    uint32_t k;                // number of sources
+    // Graphs of the run. Several disjoint graphs are joined into one
+    // block-diagonal resident graph with 32-aligned vertex offsets; source
+    // slot b of a group then holds the b-th source of EVERY graph (their
+    // vertex sets never meet). word_part maps each 32-vertex word to its
+    // graph; with parts == nullptr the run has the single graph part0.
+    const MbfsPart* parts;
+    uint32_t nparts;
+    const uint32_t* word_part;
+    MbfsPart part0;
+    const uint32_t* sources;   // local source ids, per part from src_base
+    uint32_t groups;           // ceil(max k / group_width)
     uint32_t group_width;      // sources per group (32 * WORDS)
     float pull_fraction;       // pull when frontier vertices > n * pull_fraction
 };
+
+__device__ __forceinline__ MbfsPart load_part(const MbfsArgs& a, uint32_t p) {
+    if (!a.parts) return a.part0;
+    MbfsPart P;
+    P.off = __ldg(&a.parts[p].off);
+    P.n = __ldg(&a.parts[p].n);
+    P.k = __ldg(&a.parts[p].k);
+    P.src_base = __ldg(&a.parts[p].src_base);
+    P.levels = a.parts[p].levels;
+    return P;
+}
+
+__device__ __forceinline__ uint32_t part_of_word(const MbfsArgs& a, uint32_t wi) {
+    return a.word_part ? __ldg(&a.word_part[wi]) : 0u;
+}
+
+// Sources of part P in the group starting at s0 (0 when it has none left).
+__device__ __forceinline__ uint32_t group_rows(const MbfsPart& P, uint32_t s0, uint32_t width) {
+    return P.k > s0 ? min(width, P.k - s0) : 0u;
+}
+
+template <int WORDS>
+__device__ __forceinline__ void rows_mask(uint32_t rows, uint32_t (&m)[WORDS]) {
+#pragma unroll
+    for (int w = 0; w < WORDS; ++w) {
+        const uint32_t lo = 32 * w;
+        m[w] = rows >= lo + 32 ? 0xFFFFFFFFu : (rows > lo ? ((1u << (rows - lo)) - 1) : 0u);
+    }
+}
 
 template <int WORDS>
 struct Bits {
@@ -93,60 +141,75 @@ __global__ void __launch_bounds__(512, 2) mbfs_persistent_kernel(MbfsArgs a) {
     const uint32_t Wn = (n + 31) / 32;
     auto barrier = [&]() -> bool { return grid_barrier(c); };
 
-    const uint32_t groups = (a.k + a.group_width - 1) / a.group_width;
-    for (uint32_t grp = 0; grp < groups; ++grp) {
+    for (uint32_t grp = 0; grp < a.groups; ++grp) {
         const uint32_t s0 = grp * a.group_width;
-        const uint32_t ns = min(a.group_width, a.k - s0);
-        Bits<WORDS> valid;
-#pragma unroll
-        for (int w = 0; w < WORDS; ++w) {
-            const int lo = 32 * w;
-            valid.w[w] = (int)ns >= lo + 32 ? 0xFFFFFFFFu : ((int)ns > lo ? ((1u << (ns - lo)) - 1) : 0u);
-        }
-        // ---- group init: state cleared, output rows unreached
+        // ---- group init: state cleared, output rows of the group unreached
         for (uint32_t i = tid; i < n * WORDS; i += nth) {
             a.visited[i] = 0u;
             a.frontier[i] = 0u;
             a.next[i] = 0u;
         }
-        const uint64_t outN = (uint64_t)ns * n;
-        uint32_t* out = a.levels + (uint64_t)s0 * n;
-        for (uint64_t i = tid; i < outN; i += nth) out[i] = kUnreached;
+        for (uint32_t wi = warp; wi < Wn; wi += nwarps) {
+            const MbfsPart P = load_part(a, part_of_word(a, wi));
+            const uint32_t rows = group_rows(P, s0, a.group_width);
+            const uint32_t lv = wi * 32 + lane - P.off;
+            if (lv < P.n)
+                for (uint32_t b = 0; b < rows; ++b) P.levels[(uint64_t)(s0 + b) * P.n + lv] = kUnreached;
+        }
         if (tid == 0) {
             c->aux[0] = c->aux[1] = 0;  // push queue counters (2 slots)
             c->aux[4] = c->aux[5] = 0;  // new-frontier vertex counts (2 slots)
         }
         if (!barrier()) return;
-        for (uint32_t i = tid; i < ns; i += nth) {
-            const uint32_t v = a.sources[s0 + i];
-            atomicOr(&a.visited[v * WORDS + (i >> 5)], 1u << (i & 31));
-            atomicOr(&a.frontier[v * WORDS + (i >> 5)], 1u << (i & 31));
-            out[(uint64_t)i * n + v] = 0u;
-        }
-        // queue the sources' rsets (slot 0); duplicates are harmless
-        if (warp == 0) {
-            for (uint32_t base = 0; base < ns; base += 32) {
-                const uint32_t i = base + lane;
+        // ---- seeds: pair t = (part t / width, slot t % width); the sources'
+        // rsets are queued in slot 0 (duplicates are harmless)
+        {
+            const uint32_t pairs = a.nparts * a.group_width;
+            uint32_t seeded = 0;
+            for (uint32_t base = warp * 32; base < pairs; base += nwarps * 32) {
+                const uint32_t t = base + lane;
+                const uint32_t p = t / a.group_width, b = t % a.group_width;
                 uint32_t r = 0, units = 0;
-                if (i < ns) {
-                    r = a.sources[s0 + i] >> 3;
-                    const uint32_t t = __ldg(&g.rset_tile[r + 1]) - __ldg(&g.rset_tile[r]);
-                    units = (t + 31) / 32;
+                if (p < a.nparts) {
+                    const MbfsPart P = load_part(a, p);
+                    if (b < group_rows(P, s0, a.group_width)) {
+                        const uint32_t src = __ldg(&a.sources[P.src_base + s0 + b]);
+                        if (src >= P.n) {
+                            set_error(c, BLEST_ERR_DEVICE_INDEX);
+                        } else {
+                            const uint32_t v = P.off + src;
+                            atomicOr(&a.visited[v * WORDS + (b >> 5)], 1u << (b & 31));
+                            atomicOr(&a.frontier[v * WORDS + (b >> 5)], 1u << (b & 31));
+                            P.levels[(uint64_t)(s0 + b) * P.n + src] = 0u;
+                            ++seeded;
+                            r = v >> 3;
+                            const uint32_t tl = __ldg(&g.rset_tile[r + 1]) - __ldg(&g.rset_tile[r]);
+                            units = (tl + 31) / 32;
+                        }
+                    }
                 }
-                const bool enq = units > 0;
-                const uint64_t mine = enq ? ((1ull << kQShift) | units) : 0ull;
+                const uint64_t mine = units ? ((1ull << kQShift) | units) : 0ull;
                 const uint64_t incl = warp_inclusive_scan64(mine);
-                uint64_t b0 = 0;
-                if (lane == 31) b0 = atomicAdd(&c->aux[0], (unsigned long long)incl);
-                b0 = __shfl_sync(0xFFFFFFFFu, b0, 31);
-                if (enq) {
-                    const uint64_t ex = b0 + incl - mine;
-                    a.q_rset[(uint32_t)(ex >> kQShift)] = r;
-                    a.q_off[(uint32_t)(ex >> kQShift)] = (uint32_t)(ex & kQUnitMask);
+                const uint64_t tot = __shfl_sync(0xFFFFFFFFu, incl, 31);
+                if (tot) {
+                    uint64_t b0 = 0;
+                    if (lane == 31) b0 = atomicAdd(&c->aux[0], (unsigned long long)tot);
+                    b0 = __shfl_sync(0xFFFFFFFFu, b0, 31);
+                    if (mine) {
+                        const uint64_t ex = b0 + incl - mine;
+                        const uint32_t e = (uint32_t)(ex >> kQShift);
+                        if (e < a.qreg) {
+                            a.q_rset[e] = r;
+                            a.q_off[e] = (uint32_t)(ex & kQUnitMask);
+                        } else {
+                            set_error(c, BLEST_ERR_DEVICE_INDEX);
+                        }
+                    }
                 }
             }
+            const uint64_t ws = warp_sum64(seeded);
+            if (lane == 0 && ws) atomicAdd(&c->aux[4], (unsigned long long)ws);
         }
-        if (tid == 0) c->aux[4] = ns;
         if (!barrier()) return;
 
         for (uint32_t level = 1;; ++level) {
@@ -165,12 +228,14 @@ __global__ void __launch_bounds__(512, 2) mbfs_persistent_kernel(MbfsArgs a) {
             // ---- expand
             if (pull) {
                 for (uint32_t v = tid; v < n; v += nth) {
+                    uint32_t valid[WORDS];
+                    rows_mask<WORDS>(group_rows(load_part(a, part_of_word(a, v >> 5)), s0, a.group_width), valid);
                     const Bits<WORDS> vis = load_bits<WORDS>(a.visited, v);
                     Bits<WORDS> need, acc;
                     bool any = false;
 #pragma unroll
                     for (int w = 0; w < WORDS; ++w) {
-                        need.w[w] = ~vis.w[w] & valid.w[w];
+                        need.w[w] = ~vis.w[w] & valid[w];
                         acc.w[w] = 0u;
                         any |= need.w[w] != 0;
                     }
@@ -293,14 +358,17 @@ __global__ void __launch_bounds__(512, 2) mbfs_persistent_kernel(MbfsArgs a) {
                 const uint32_t anyMask = __ballot_sync(0xFFFFFFFFu, any);
                 if (!anyMask) continue;
                 cnt += any ? 1u : 0u;
-                // levels of the new (source, vertex) pairs, one source row at a time
+                // levels of the new (source, vertex) pairs, one source row at
+                // a time (new bits only arise in real vertices of the part)
+                const MbfsPart P = load_part(a, part_of_word(a, wi));
+                const uint32_t lv = v - P.off;
 #pragma unroll
                 for (int w = 0; w < WORDS; ++w) {
                     uint32_t rowsAny = __reduce_or_sync(0xFFFFFFFFu, nw.w[w]);
                     while (rowsAny) {
                         const uint32_t b = __ffs(rowsAny) - 1;
                         rowsAny &= rowsAny - 1;
-                        if ((nw.w[w] >> b) & 1u) out[(uint64_t)(32 * w + b) * n + v] = level;
+                        if ((nw.w[w] >> b) & 1u) P.levels[(uint64_t)(s0 + 32 * w + b) * P.n + lv] = level;
                     }
                 }
                 // queue rsets with new bits (lanes 8j..8j+7 share rset)
@@ -346,8 +414,15 @@ struct MbfsScratch {
     uint32_t* state = nullptr;  // visited | frontier | next
     uint32_t* levels = nullptr; // staging for host output
     uint32_t* sources = nullptr;
-    size_t state_words = 0, levels_words = 0, sources_cap = 0;
+    uint32_t* queue = nullptr;  // rset queue: 2 slots of entries + 2 slots of offsets
+    size_t state_words = 0, levels_words = 0, sources_cap = 0, queue_words = 0;
 };
+
+// Entries one queue slot needs: a sweep queues each rset at most once; the
+// seeding of a group queues one entry per source (duplicates allowed).
+inline uint32_t mbfs_queue_slot(uint32_t rsets, uint64_t seeds) {
+    return (uint32_t)std::min<uint64_t>(rsets + seeds + 64, 0xFFFFFFFFull / 4);
+}
 
 void ensure(uint32_t*& p, size_t& cap, size_t need) {
     if (cap >= need) return;
@@ -357,36 +432,62 @@ void ensure(uint32_t*& p, size_t& cap, size_t need) {
     cap = need;
 }
 
+// A prepared MBFS launch: arguments (graph, state, queue, counters, launch
+// geometry) filled except for the parts/sources of the run.
+struct MbfsLaunch {
+    dev::MbfsArgs a{};
+    const void* kern = nullptr;
+    int grid = 0;
+    int threads = 0;
+};
+
 template <int WORDS>
-void launch_mbfs(const blest_graph* g, blest::Workspace& w, MbfsScratch& sc, const uint32_t* dsrc, uint32_t k,
-                 uint32_t* dlevels, const blest_mbfs_params& p, cudaStream_t s) {
+void prepare_words(const blest_graph* g, blest::Workspace& w, MbfsScratch& sc, const blest_mbfs_params& p,
+                   uint64_t seeds, MbfsLaunch& L) {
     const uint32_t n = g->d.n;
     ensure(sc.state, sc.state_words, 3ull * n * WORDS);
-    dev::MbfsArgs a{};
+    dev::MbfsArgs& a = L.a;
     a.g = g->d;
     a.visited = sc.state;
     a.frontier = sc.state + (size_t)n * WORDS;
     a.next = sc.state + 2ull * n * WORDS;
-    a.qreg = w.qcap / 2;
-    if (a.qreg < g->d.no_real) throw Error(BLEST_ERR_UNSUPPORTED, "workspace queue too small for MBFS");
-    a.q_rset = w.q_rset;
-    a.q_off = w.q_off;
+    a.qreg = mbfs_queue_slot(g->d.no_real, seeds);
+    ensure(sc.queue, sc.queue_words, 4ull * a.qreg);
+    a.q_rset = sc.queue;
+    a.q_off = sc.queue + 2ull * a.qreg;
     a.ctr = w.counters;
-    a.levels = dlevels;
-    a.sources = dsrc;
-    a.k = k;
     a.group_width = 32 * WORDS;
-    a.pull_fraction = 1.0f / 64.0f;
-    const int threads = p.threads_per_block > 0 ? p.threads_per_block : 512;
+    a.pull_fraction = p.pull_fraction > 0 ? (float)p.pull_fraction : 1.0f / 64.0f;
+    L.threads = p.threads_per_block > 0 ? p.threads_per_block : 512;
+    if (L.threads % 32 || L.threads > 512) throw Error(BLEST_ERR_INVALID_ARG, "threads_per_block must be a multiple of 32, <= 512");
     auto kern = dev::mbfs_persistent_kernel<WORDS>;
+    L.kern = (const void*)kern;
     int maxBlocks = 0;
-    BLEST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxBlocks, kern, threads, 0));
+    BLEST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxBlocks, kern, L.threads, 0));
     if (maxBlocks < 1) throw Error(BLEST_ERR_CUDA, "MBFS kernel cannot be resident");
     const int bps = p.blocks_per_sm > 0 ? std::min(p.blocks_per_sm, maxBlocks) : maxBlocks;
-    BLEST_CUDA(cudaMemsetAsync(a.ctr, 0, sizeof(dev::RunCounters), s));
+    L.grid = cooperative_grid(bps, g->sm_count, w.grid_blocks);
+}
+
+// `seeds`: the most sources one group seeds (sum over graphs of their
+// sources in a group), which sizes the rset queue.
+MbfsLaunch prepare_mbfs(const blest_graph* g, blest::Workspace& w, MbfsScratch& sc, const blest_mbfs_params& p,
+                        uint64_t seeds) {
+    MbfsLaunch L;
+    const uint32_t gw = p.group_width ? p.group_width : 128;
+    if (gw == 128) prepare_words<4>(g, w, sc, p, seeds, L);
+    else if (gw == 64) prepare_words<2>(g, w, sc, p, seeds, L);
+    else if (gw == 32) prepare_words<1>(g, w, sc, p, seeds, L);
+    else throw Error(BLEST_ERR_INVALID_ARG, "group_width must be 32, 64 or 128");
+    return L;
+}
+
+// Counters reset + the cooperative launch (both capturable into a graph).
+void issue_mbfs(const MbfsLaunch& L, cudaStream_t s) {
+    BLEST_CUDA(cudaMemsetAsync(L.a.ctr, 0, sizeof(dev::RunCounters), s));
+    dev::MbfsArgs a = L.a;
     void* kargs[] = {(void*)&a};
-    BLEST_CUDA(cudaLaunchCooperativeKernel((void*)kern, cooperative_grid(bps, g->sm_count, w.grid_blocks), threads,
-                                           kargs, 0, s));
+    BLEST_CUDA(cudaLaunchCooperativeKernel(L.kern, L.grid, L.threads, kargs, 0, s));
 }
 
 }  // namespace
@@ -396,6 +497,7 @@ void mbfs_reserve(Workspace& w, uint32_t n, uint32_t words) {
     MbfsScratch& sc = *(MbfsScratch*)w.mbfs;
     ensure(sc.state, sc.state_words, 3ull * n * words);
     ensure(sc.sources, sc.sources_cap, 128);
+    ensure(sc.queue, sc.queue_words, 4ull * mbfs_queue_slot((n + 7) / 8, 32u * words));
 }
 
 void mbfs_scratch_free(void* p) {
@@ -404,12 +506,214 @@ void mbfs_scratch_free(void* p) {
     cudaFree(sc->state);
     cudaFree(sc->levels);
     cudaFree(sc->sources);
+    cudaFree(sc->queue);
     delete sc;
 }
+
+// ---------------------------------------------------------------------------
+// Multi-graph runs: the items' device graphs are joined into one
+// block-diagonal graph by one copy kernel over a table of segments (each an
+// array slice copied with an id offset added, or a fill).
+namespace dev {
+
+struct JoinSeg {
+    const void* src;
+    void* dst;
+    uint64_t count;
+    uint64_t add;
+    uint32_t kind;  // JoinKind
+    uint32_t pad;
+};
+enum JoinKind : uint32_t { kAdd32 = 0, kAdd32KeepPad = 1, kAdd64 = 2, kFill32 = 3, kFill64 = 4 };
+
+// blockIdx.y = segment (of this chunk of the table); the x blocks stride it.
+__global__ void join_kernel(const JoinSeg* segs) {
+    const JoinSeg sg = segs[blockIdx.y];
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < sg.count; i += stride) {
+        switch (sg.kind) {
+        case kAdd32:
+            static_cast<uint32_t*>(sg.dst)[i] = static_cast<const uint32_t*>(sg.src)[i] + (uint32_t)sg.add;
+            break;
+        case kAdd32KeepPad: {
+            const uint32_t x = static_cast<const uint32_t*>(sg.src)[i];
+            static_cast<uint32_t*>(sg.dst)[i] = x == kUnreached ? x : x + (uint32_t)sg.add;
+            break;
+        }
+        case kAdd64:
+            static_cast<uint64_t*>(sg.dst)[i] = static_cast<const uint64_t*>(sg.src)[i] + sg.add;
+            break;
+        case kFill32:
+            static_cast<uint32_t*>(sg.dst)[i] = (uint32_t)sg.add;
+            break;
+        default:
+            static_cast<uint64_t*>(sg.dst)[i] = sg.add;
+            break;
+        }
+    }
+}
+
+}  // namespace dev
+
+namespace {
+
+template <class T>
+T* plan_alloc(blest_graph* u, size_t count) {
+    void* p = nullptr;
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    BLEST_CUDA(cudaMalloc(&p, bytes));
+    u->allocations.push_back(p);
+    u->graph_bytes += bytes;
+    return (T*)p;
+}
+
+// Join the graphs into `u` (device arrays) with vertex offsets off[i]
+// (multiples of 32; graph i padded with isolated vertices to a multiple
+// of 32). Every index array gets its graph's offset in the joined space.
+void join_graphs(const std::vector<const blest_graph*>& gs, const std::vector<uint32_t>& off, uint32_t N,
+                 blest_graph* u, cudaStream_t s) {
+    using dev::JoinSeg;
+    uint64_t V = 0, T = 0, E = 0;
+    for (auto* g : gs) {
+        V += g->d.no_virtual;
+        T += g->d.no_slices / 4;
+        E += g->d.nnz;
+    }
+    if (V >= 0xFFFFFFFFull || T >= 0xFFFFFFFFull || E >= 0xFFFFFFFFull)
+        throw Error(BLEST_ERR_UNSUPPORTED, "joined graph exceeds 2^32 vertex sets, tiles or edges");
+    const uint32_t R = N / 8;
+    dev::DevGraph& d = u->d;
+    d.n = N;
+    d.no_real = R;
+    d.no_virtual = (uint32_t)V;
+    d.no_slices = 4 * T;
+    d.nnz = (uint32_t)E;
+    d.degree_total = E;
+    uint64_t* ssp = plan_alloc<uint64_t>(u, V + 1);
+    uint32_t* v2r = plan_alloc<uint32_t>(u, V);
+    uint32_t* rp = plan_alloc<uint32_t>(u, (size_t)R + 1);
+    uint32_t* rows = plan_alloc<uint32_t>(u, 4 * T);
+    uint32_t* masks = plan_alloc<uint32_t>(u, T);
+    uint32_t* rt = plan_alloc<uint32_t>(u, (size_t)R + 1);
+    uint32_t* cp = plan_alloc<uint32_t>(u, (size_t)N + 1);
+    uint32_t* ci = plan_alloc<uint32_t>(u, E);
+    uint32_t* hin = plan_alloc<uint32_t>(u, (size_t)N / 32 + 4);
+    std::vector<JoinSeg> segs;
+    auto seg = [&](const void* src, void* dst, uint64_t count, uint64_t add, uint32_t kind) {
+        if (count) segs.push_back(JoinSeg{src, dst, count, add, kind, 0});
+    };
+    uint64_t vo = 0, to = 0, eo = 0;
+    for (size_t i = 0; i < gs.size(); ++i) {
+        const dev::DevGraph& g = gs[i]->d;
+        const uint32_t o = off[i], ri = g.no_real, rpad = (o + ((g.n + 31) & ~31u)) / 8 - o / 8;
+        const uint64_t ti = g.no_slices / 4;
+        seg(g.slice_set_ptrs, ssp + vo, g.no_virtual, 4 * to, dev::kAdd64);
+        seg(g.virtual_to_real, v2r + vo, g.no_virtual, o / 8, dev::kAdd32);
+        seg(g.real_ptrs, rp + o / 8, ri, vo, dev::kAdd32);
+        seg(nullptr, rp + o / 8 + ri, rpad - ri, vo + g.no_virtual, dev::kFill32);
+        seg(g.row4, rows + 4 * to, 4 * ti, o, dev::kAdd32KeepPad);
+        seg(g.masks, masks + to, ti, 0, dev::kAdd32);
+        seg(g.rset_tile, rt + o / 8, ri, to, dev::kAdd32);
+        seg(nullptr, rt + o / 8 + ri, rpad - ri, to + ti, dev::kFill32);
+        seg(g.csr_ptrs, cp + o, g.n, eo, dev::kAdd32);
+        seg(nullptr, cp + o + g.n, ((g.n + 31) & ~31u) - g.n, eo + g.nnz, dev::kFill32);
+        seg(g.csr_ids, ci + eo, g.nnz, o, dev::kAdd32);
+        if (g.has_in) seg(g.has_in, hin + o / 32, (g.n + 31) / 32, 0, dev::kAdd32);
+        else seg(nullptr, hin + o / 32, (g.n + 31) / 32, 0xFFFFFFFFull, dev::kFill32);
+        vo += g.no_virtual;
+        to += ti;
+        eo += g.nnz;
+    }
+    seg(nullptr, ssp + V, 1, 4 * T, dev::kFill64);
+    seg(nullptr, rp + R, 1, V, dev::kFill32);
+    seg(nullptr, rt + R, 1, T, dev::kFill32);
+    seg(nullptr, cp + N, 1, E, dev::kFill32);
+    seg(nullptr, hin + N / 32, 4, 0, dev::kFill32);
+    JoinSeg* dsegs = nullptr;
+    BLEST_CUDA(cudaMalloc((void**)&dsegs, segs.size() * sizeof(JoinSeg)));
+    const cudaError_t e1 = cudaMemcpyAsync(dsegs, segs.data(), segs.size() * sizeof(JoinSeg), cudaMemcpyHostToDevice, s);
+    for (size_t b = 0; e1 == cudaSuccess && b < segs.size(); b += 65535) {
+        const unsigned ny = (unsigned)std::min<size_t>(65535, segs.size() - b);
+        dev::join_kernel<<<dim3(64, ny), 256, 0, s>>>(dsegs + b);
+    }
+    const cudaError_t e2 = cudaStreamSynchronize(s);
+    cudaFree(dsegs);
+    BLEST_CUDA(e1);
+    BLEST_CUDA(cudaGetLastError());
+    BLEST_CUDA(e2);
+    d.slice_set_ptrs = ssp;
+    d.virtual_to_real = v2r;
+    d.real_ptrs = rp;
+    d.row4 = (const uint4*)rows;
+    d.masks = masks;
+    d.rset_tile = rt;
+    d.csr_ptrs = cp;
+    d.csr_ids = ci;
+    d.has_in = hin;
+    u->undirected_edges = E / 2;
+}
+
+}  // namespace
 
 }  // namespace blest
 
 using blest::guarded;
+
+struct blest_mbfs_plan {
+    int device = 0;
+    blest_graph* u = nullptr;       // the joined graph
+    blest_workspace* ws = nullptr;  // its workspace
+    blest::dev::MbfsPart* d_parts = nullptr;
+    uint32_t* d_word_part = nullptr;
+    uint32_t* d_sources = nullptr;
+    std::vector<blest::dev::MbfsPart> parts;  // host copy
+    blest_mbfs_params params{};
+    blest::MbfsLaunch L;
+    cudaStream_t stream = nullptr;
+    bool owns_stream = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool captured = false;
+    bool pending = false;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    uint64_t table_bytes = 0;
+};
+
+namespace {
+
+void plan_free(blest_mbfs_plan* p) {
+    if (!p) return;
+    cudaSetDevice(p->device);
+    if (p->stream) cudaStreamSynchronize(p->stream);
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    cudaFree(p->d_parts);
+    cudaFree(p->d_word_part);
+    cudaFree(p->d_sources);
+    if (p->ws) {
+        blest::workspace_free(p->ws->w);
+        delete p->ws;
+    }
+    if (p->u) blest_graph_destroy(p->u);
+    if (p->e0) cudaEventDestroy(p->e0);
+    if (p->e1) cudaEventDestroy(p->e1);
+    if (p->stream && p->owns_stream) cudaStreamDestroy(p->stream);
+    delete p;
+}
+
+// The run as stream work: counter reset, cooperative launch, status copy.
+void plan_issue(blest_mbfs_plan* p) {
+    blest::issue_mbfs(p->L, p->stream);
+    BLEST_CUDA(cudaMemcpyAsync(p->ws->w.host_counters, p->ws->w.counters, sizeof(blest::dev::RunCounters),
+                               cudaMemcpyDeviceToHost, p->stream));
+}
+
+void check_sources(const blest_mbfs_item& it, uint32_t n) {
+    for (uint32_t j = 0; j < it.k; ++j)
+        if (it.sources[j] >= n) throw blest::Error(BLEST_ERR_INVALID_ARG, "source vertex out of range");
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -439,10 +743,15 @@ int blest_mbfs_ws(blest_workspace* ws, const uint32_t* sources, uint32_t k, uint
             blest::ensure(sc.levels, sc.levels_words, (size_t)k * n);
             dl = sc.levels;
         }
+        blest::MbfsLaunch L = blest::prepare_mbfs(g, w, sc, p, std::min(k, gw));
+        L.a.parts = nullptr;
+        L.a.nparts = 1;
+        L.a.word_part = nullptr;
+        L.a.part0 = blest::dev::MbfsPart{0u, n, k, 0u, dl};
+        L.a.sources = sc.sources;
+        L.a.groups = (k + gw - 1) / gw;
         BLEST_CUDA(cudaEventRecord(w.ev_start, s));
-        if (gw == 128) blest::launch_mbfs<4>(g, w, sc, sc.sources, k, dl, p, s);
-        else if (gw == 64) blest::launch_mbfs<2>(g, w, sc, sc.sources, k, dl, p, s);
-        else blest::launch_mbfs<1>(g, w, sc, sc.sources, k, dl, p, s);
+        blest::issue_mbfs(L, s);
         BLEST_CUDA(cudaEventRecord(w.ev_stop, s));
         BLEST_CUDA(cudaMemcpyAsync(w.host_counters, w.counters, sizeof(blest::dev::RunCounters),
                                    cudaMemcpyDeviceToHost, s));
@@ -473,28 +782,223 @@ int blest_mbfs(blest_graph* g, const uint32_t* sources, uint32_t k, uint32_t* le
     return blest_mbfs_ws(g->default_ws, sources, k, levels_out, out_mem, params, g->stream, stats);
 }
 
+
+int blest_mbfs_plan_create(const blest_mbfs_item* items, uint32_t count, const blest_mbfs_params* params,
+                           void* stream, blest_mbfs_plan** out) {
+    blest_mbfs_plan* p = nullptr;
+    const int rc = guarded([&] {
+        blest::require(items && count && out, "null argument or empty batch");
+        const int dev = items[0].graph ? items[0].graph->device : 0;
+        std::vector<const blest_graph*> gs(count);
+        std::vector<uint32_t> off(count);
+        uint64_t N = 0, K = 0;
+        uint32_t maxk = 0;
+        for (uint32_t i = 0; i < count; ++i) {
+            const blest_mbfs_item& it = items[i];
+            blest::require(it.graph, "null graph in batch");
+            blest::require(it.graph->device == dev, "batch graphs must be on one device");
+            blest::require(it.k == 0 || (it.sources && it.levels_out), "null sources or levels_out");
+            check_sources(it, it.graph->d.n);
+            gs[i] = it.graph;
+            off[i] = (uint32_t)std::min<uint64_t>(N, 0xFFFFFFFFull);
+            N += (it.graph->d.n + 31ull) & ~31ull;
+            K += it.k;
+            maxk = std::max(maxk, it.k);
+        }
+        if (N >= (1ull << 28)) throw blest::Error(BLEST_ERR_UNSUPPORTED, "joined graph has 2^28 or more vertices");
+        blest_mbfs_params prm{};
+        if (params) prm = *params;
+        if (!prm.group_width) prm.group_width = 128;
+        BLEST_CUDA(cudaSetDevice(dev));
+        p = new blest_mbfs_plan;
+        p->device = dev;
+        p->params = prm;
+        if (stream) {
+            p->stream = (cudaStream_t)stream;
+        } else {
+            BLEST_CUDA(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+            p->owns_stream = true;
+        }
+        p->u = new blest_graph;
+        p->u->device = dev;
+        p->u->sm_count = gs[0]->sm_count;
+        p->u->stream = p->stream;
+        blest::join_graphs(gs, off, (uint32_t)N, p->u, p->stream);
+        p->ws = new blest_workspace;
+        p->ws->g = p->u;
+        blest::workspace_alloc(p->u, p->ws->w);
+        p->ws->w.mbfs = new blest::MbfsScratch;
+        // parts, word -> part map, sources
+        std::vector<uint32_t> wordPart(N / 32);
+        std::vector<uint32_t> src(std::max<uint64_t>(K, 1));
+        uint32_t base = 0;
+        p->parts.resize(count);
+        for (uint32_t i = 0; i < count; ++i) {
+            const uint32_t n = gs[i]->d.n;
+            p->parts[i] = blest::dev::MbfsPart{off[i], n, items[i].k, base, items[i].levels_out};
+            std::fill(wordPart.begin() + off[i] / 32, wordPart.begin() + off[i] / 32 + (n + 31) / 32, i);
+            std::copy(items[i].sources, items[i].sources + items[i].k, src.begin() + base);
+            base += items[i].k;
+        }
+        BLEST_CUDA(cudaMalloc((void**)&p->d_parts, sizeof(blest::dev::MbfsPart) * count));
+        BLEST_CUDA(cudaMalloc((void**)&p->d_word_part, 4ull * wordPart.size()));
+        BLEST_CUDA(cudaMalloc((void**)&p->d_sources, 4ull * src.size()));
+        p->table_bytes = sizeof(blest::dev::MbfsPart) * count + 4ull * wordPart.size() + 4ull * src.size();
+        BLEST_CUDA(cudaMemcpy(p->d_parts, p->parts.data(), sizeof(blest::dev::MbfsPart) * count, cudaMemcpyHostToDevice));
+        BLEST_CUDA(cudaMemcpy(p->d_word_part, wordPart.data(), 4ull * wordPart.size(), cudaMemcpyHostToDevice));
+        BLEST_CUDA(cudaMemcpy(p->d_sources, src.data(), 4ull * src.size(), cudaMemcpyHostToDevice));
+        blest::MbfsScratch& sc = *(blest::MbfsScratch*)p->ws->w.mbfs;
+        uint64_t seeds = 0;
+        for (uint32_t i = 0; i < count; ++i) seeds += std::min(items[i].k, prm.group_width);
+        p->L = blest::prepare_mbfs(p->u, p->ws->w, sc, prm, seeds);
+        p->L.a.parts = p->d_parts;
+        p->L.a.nparts = count;
+        p->L.a.word_part = p->d_word_part;
+        p->L.a.part0 = p->parts[0];
+        p->L.a.sources = p->d_sources;
+        p->L.a.groups = (maxk + prm.group_width - 1) / prm.group_width;
+        BLEST_CUDA(cudaEventCreate(&p->e0));
+        BLEST_CUDA(cudaEventCreate(&p->e1));
+        // Capture the run into a CUDA graph; if this driver cannot capture
+        // it, the plan replays the same stream work directly (info.captured).
+        BLEST_CUDA(cudaStreamSynchronize(p->stream));
+        if (cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            bool ok = true;
+            try {
+                plan_issue(p);
+            } catch (const blest::Error&) {
+                ok = false;
+            }
+            cudaGraph_t gr = nullptr;
+            ok = cudaStreamEndCapture(p->stream, &gr) == cudaSuccess && ok && gr;
+            if (ok && cudaGraphInstantiate(&p->exec, gr, 0) == cudaSuccess) {
+                p->graph = gr;
+                p->captured = true;
+            } else if (gr) {
+                cudaGraphDestroy(gr);
+            }
+        }
+        (void)cudaGetLastError();
+        *out = p;
+    });
+    if (rc != BLEST_OK && p) plan_free(p);
+    return rc;
+}
+
+int blest_mbfs_plan_set_sources(blest_mbfs_plan* p, uint32_t item, const uint32_t* sources) {
+    return guarded([&] {
+        blest::require(p && (sources || (item < p->parts.size() && p->parts[item].k == 0)), "null argument");
+        blest::require(item < p->parts.size(), "item index out of range");
+        const blest::dev::MbfsPart& P = p->parts[item];
+        for (uint32_t j = 0; j < P.k; ++j)
+            if (sources[j] >= P.n) throw blest::Error(BLEST_ERR_INVALID_ARG, "source vertex out of range");
+        BLEST_CUDA(cudaSetDevice(p->device));
+        if (P.k)
+            BLEST_CUDA(cudaMemcpyAsync(p->d_sources + P.src_base, sources, 4ull * P.k, cudaMemcpyHostToDevice, p->stream));
+    });
+}
+
+int blest_mbfs_plan_launch(blest_mbfs_plan* p) {
+    return guarded([&] {
+        blest::require(p, "null argument");
+        BLEST_CUDA(cudaSetDevice(p->device));
+        BLEST_CUDA(cudaEventRecord(p->e0, p->stream));
+        if (p->captured) BLEST_CUDA(cudaGraphLaunch(p->exec, p->stream));
+        else plan_issue(p);
+        BLEST_CUDA(cudaEventRecord(p->e1, p->stream));
+        p->pending = true;
+    });
+}
+
+int blest_mbfs_plan_sync(blest_mbfs_plan* p, blest_mbfs_stats* stats) {
+    return guarded([&] {
+        blest::require(p, "null argument");
+        if (!p->pending) throw blest::Error(BLEST_ERR_INVALID_ARG, "no run pending");
+        BLEST_CUDA(cudaSetDevice(p->device));
+        BLEST_CUDA(cudaStreamSynchronize(p->stream));
+        p->pending = false;
+        const blest::dev::RunCounters& c = *p->ws->w.host_counters;
+        if (c.error)
+            throw blest::Error((int)c.error, c.error == BLEST_ERR_BARRIER_TIMEOUT ? "device grid barrier timed out"
+                                                                                 : "MBFS device error");
+        float ms = 0;
+        BLEST_CUDA(cudaEventElapsedTime(&ms, p->e0, p->e1));
+        if (stats) {
+            stats->time = ms * 1e-3;
+            stats->groups = p->L.a.groups;
+            stats->max_levels = c.levels + 1;
+            stats->reached_degree_sum = 0;
+        }
+    });
+}
+
+int blest_mbfs_plan_run(blest_mbfs_plan* p, blest_mbfs_stats* stats) {
+    const int rc = blest_mbfs_plan_launch(p);
+    return rc != BLEST_OK ? rc : blest_mbfs_plan_sync(p, stats);
+}
+
+int blest_mbfs_plan_info_get(const blest_mbfs_plan* p, blest_mbfs_plan_info* out) {
+    return guarded([&] {
+        blest::require(p && out, "null argument");
+        out->items = (uint32_t)p->parts.size();
+        out->n = p->u->d.n;
+        out->nnz = p->u->d.nnz;
+        out->no_slices = p->u->d.no_slices;
+        out->groups = p->L.a.groups;
+        out->group_width = p->L.a.group_width;
+        out->grid_blocks = p->L.grid;
+        out->captured = p->captured ? 1 : 0;
+        const blest::MbfsScratch& sc = *(const blest::MbfsScratch*)p->ws->w.mbfs;
+        out->device_bytes = p->u->graph_bytes + p->ws->w.bytes + 4ull * sc.state_words + p->table_bytes;
+    });
+}
+
+int blest_mbfs_plan_destroy(blest_mbfs_plan* p) {
+    plan_free(p);
+    return BLEST_OK;
+}
+
 int blest_mbfs_batch(const blest_mbfs_item* items, uint32_t count, int out_mem, const blest_mbfs_params* params,
                      void* stream, blest_mbfs_stats* stats) {
     return guarded([&] {
         blest::require(items || count == 0, "null argument");
-        double total = 0;
-        uint32_t groups = 0, maxl = 0;
-        for (uint32_t i = 0; i < count; ++i) {
-            blest_mbfs_stats st{};
-            const int rc = blest_mbfs(items[i].graph, items[i].sources, items[i].k, items[i].levels_out, out_mem,
-                                      params, &st);
-            if (rc != BLEST_OK) throw blest::Error(rc, blest_last_error());
-            total += st.time;
-            groups += st.groups;
-            maxl = std::max(maxl, st.max_levels);
+        blest::require(out_mem == BLEST_MEM_HOST || out_mem == BLEST_MEM_DEVICE, "bad out_mem");
+        if (count == 0) {
+            if (stats) *stats = blest_mbfs_stats{};
+            return;
         }
-        (void)stream;
-        if (stats) {
-            stats->time = total;
-            stats->groups = groups;
-            stats->max_levels = maxl;
-            stats->reached_degree_sum = 0;
+        std::vector<blest_mbfs_item> dev(items, items + count);
+        uint32_t* staging = nullptr;
+        if (out_mem == BLEST_MEM_HOST) {
+            uint64_t total = 0;
+            for (uint32_t i = 0; i < count; ++i) {
+                blest::require(items[i].graph, "null graph in batch");
+                total += (uint64_t)items[i].k * items[i].graph->d.n;
+            }
+            BLEST_CUDA(cudaSetDevice(items[0].graph->device));
+            BLEST_CUDA(cudaMalloc((void**)&staging, std::max<uint64_t>(total, 1) * 4));
+            uint64_t o = 0;
+            for (uint32_t i = 0; i < count; ++i) {
+                dev[i].levels_out = staging + o;
+                o += (uint64_t)items[i].k * items[i].graph->d.n;
+            }
         }
+        blest_mbfs_plan* plan = nullptr;
+        int rc = blest_mbfs_plan_create(dev.data(), count, params, stream, &plan);
+        if (rc == BLEST_OK) rc = blest_mbfs_plan_run(plan, stats);
+        std::string err = rc != BLEST_OK ? std::string(blest_last_error()) : std::string();
+        if (rc == BLEST_OK && out_mem == BLEST_MEM_HOST) {
+            for (uint32_t i = 0; i < count && rc == BLEST_OK; ++i)
+                if (items[i].k && cudaMemcpy(items[i].levels_out, dev[i].levels_out,
+                                             4ull * items[i].k * items[i].graph->d.n,
+                                             cudaMemcpyDeviceToHost) != cudaSuccess) {
+                    rc = BLEST_ERR_CUDA;
+                    err = "copying batch levels to the host failed";
+                }
+        }
+        blest_mbfs_plan_destroy(plan);
+        if (staging) cudaFree(staging);
+        if (rc != BLEST_OK) throw blest::Error(rc, err);
     });
 }
 

@@ -14,6 +14,15 @@ _ORDER_MODES = {"auto": L.ORDER_AUTO, "natural": L.ORDER_NATURAL, "jaccard": L.O
                 "gorder": L.ORDER_GORDER}
 
 
+def _destroy(name: str, h) -> None:
+    """Free a handle; at interpreter shutdown the bindings may already be
+    gone, and the process exit releases the memory anyway."""
+    try:
+        L.fn[name](h)
+    except (TypeError, AttributeError, KeyError):
+        pass
+
+
 def _u32p(a: np.ndarray):
     assert a.dtype == np.uint32 and a.flags.c_contiguous
     return a.ctypes.data_as(L.P(L.u32))
@@ -41,7 +50,7 @@ class Csc:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            L.fn["blest_csc_destroy"](h)
+            _destroy("blest_csc_destroy", h)
             self._h = None
 
     @staticmethod
@@ -180,7 +189,7 @@ class Bvss:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            L.fn["blest_bvss_destroy"](h)
+            _destroy("blest_bvss_destroy", h)
             self._h = None
 
     @classmethod
@@ -306,7 +315,7 @@ class Graph:
     def close(self) -> None:
         h = getattr(self, "_h", None)
         if h:
-            L.fn["blest_graph_destroy"](h)
+            _destroy("blest_graph_destroy", h)
             self._h = None
 
     __del__ = close
@@ -357,11 +366,12 @@ class Graph:
         L.call("blest_cc", self._h, lab.ctypes.data, L.MEM_HOST, C.byref(st))
         return lab, CcStats(st.time, st.no_components, st.iterations)
 
-    def mbfs(self, sources, group_width: int = 128, blocks_per_sm: int = 0, threads_per_block: int = 0):
+    def mbfs(self, sources, group_width: int = 128, blocks_per_sm: int = 0, threads_per_block: int = 0,
+             pull_fraction: float = 0.0):
         """Multi-source BFS: returns (levels[k, n], MbfsStats)."""
         src = np.ascontiguousarray(sources, dtype=np.uint32)
         out = np.empty((src.size, self.n), dtype=np.uint32)
-        p = L.MbfsParams(group_width, blocks_per_sm, threads_per_block)
+        p = L.MbfsParams(group_width, blocks_per_sm, threads_per_block, pull_fraction)
         st = L.MbfsStats()
         L.call("blest_mbfs", self._h, _u32p(src), src.size, out.ctypes.data, L.MEM_HOST, C.byref(p), C.byref(st))
         return out, MbfsStats(st.time, st.groups, st.max_levels, st.reached_degree_sum)
@@ -388,7 +398,7 @@ class Workspace:
     def close(self) -> None:
         h = getattr(self, "_h", None)
         if h:
-            L.fn["blest_workspace_destroy"](h)
+            _destroy("blest_workspace_destroy", h)
             self._h = None
 
     __del__ = close
@@ -417,3 +427,67 @@ class Workspace:
         st = L.CcStats()
         L.call("blest_cc_ws", self._h, labels_ptr, out_mem, stream, C.byref(st))
         return CcStats(st.time, st.no_components, st.iterations)
+
+
+class MbfsPlan:
+    """Multi-graph multi-source BFS in one persistent launch, replayed from a
+    captured CUDA graph (blest_mbfs_plan_*). `items` is a list of
+    (Graph, sources, levels_ptr): levels_ptr is device memory holding
+    k * n uint32 levels (source-major) for that graph."""
+
+    def __init__(self, items, group_width: int = 32, blocks_per_sm: int = 0, threads_per_block: int = 0,
+                 pull_fraction: float = 0.0, stream: int | None = None):
+        self._srcs = [np.ascontiguousarray(s, dtype=np.uint32) for _, s, _ in items]
+        arr = (L.MbfsItem * len(items))()
+        for i, ((g, _, ptr), src) in enumerate(zip(items, self._srcs)):
+            arr[i] = L.MbfsItem(g._h, _u32p(src), src.size, ptr)
+        self.graphs = [g for g, _, _ in items]
+        p = L.MbfsParams(group_width, blocks_per_sm, threads_per_block, pull_fraction)
+        h = C.c_void_p()
+        L.call("blest_mbfs_plan_create", arr, len(items), C.byref(p), stream, C.byref(h))
+        self._h = h
+
+    def set_sources(self, item: int, sources) -> None:
+        src = np.ascontiguousarray(sources, dtype=np.uint32)
+        L.call("blest_mbfs_plan_set_sources", self._h, item, _u32p(src))
+
+    def run(self) -> MbfsStats:
+        st = L.MbfsStats()
+        L.call("blest_mbfs_plan_run", self._h, C.byref(st))
+        return MbfsStats(st.time, st.groups, st.max_levels, st.reached_degree_sum)
+
+    def launch(self) -> None:
+        L.call("blest_mbfs_plan_launch", self._h)
+
+    def sync(self) -> MbfsStats:
+        st = L.MbfsStats()
+        L.call("blest_mbfs_plan_sync", self._h, C.byref(st))
+        return MbfsStats(st.time, st.groups, st.max_levels, st.reached_degree_sum)
+
+    def info(self) -> L.MbfsPlanInfo:
+        i = L.MbfsPlanInfo()
+        L.call("blest_mbfs_plan_info_get", self._h, C.byref(i))
+        return i
+
+    def close(self) -> None:
+        h = getattr(self, "_h", None)
+        if h:
+            _destroy("blest_mbfs_plan_destroy", h)
+            self._h = None
+
+    __del__ = close
+
+
+def mbfs_batch(items, out_mem: int = L.MEM_HOST, group_width: int = 32, blocks_per_sm: int = 0,
+               pull_fraction: float = 0.0) -> MbfsStats:
+    """blest_mbfs_batch over [(Graph, sources, levels)] where levels is a
+    (k, n) uint32 numpy array (out_mem host) or a device pointer."""
+    srcs = [np.ascontiguousarray(s, dtype=np.uint32) for _, s, _ in items]
+    arr = (L.MbfsItem * len(items))()
+    for i, ((g, _, out), src) in enumerate(zip(items, srcs)):
+        ptr = out.ctypes.data if isinstance(out, np.ndarray) else out
+        arr[i] = L.MbfsItem(g._h, _u32p(src), src.size, ptr)
+    p = L.MbfsParams(group_width, blocks_per_sm, 0, pull_fraction)
+    st = L.MbfsStats()
+    L.call("blest_mbfs_batch", arr, len(items), out_mem, C.byref(p), None, C.byref(st))
+    return MbfsStats(st.time, st.groups, st.max_levels, st.reached_degree_sum)

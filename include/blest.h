@@ -342,7 +342,9 @@ int blest_cc_relabel_dense(const uint32_t* labels, uint32_t n, uint32_t* dense_o
 typedef struct blest_mbfs_params {
     uint32_t group_width;     /* 32, 64 or 128 sources per pass (0 = 128) */
     int blocks_per_sm;        /* 0 = occupancy maximum */
-    int threads_per_block;    /* 0 = 256 */
+    int threads_per_block;    /* 0 = 512 */
+    double pull_fraction;     /* a level pulls when its frontier has more than
+                                 n * pull_fraction vertices (0 = 1/64) */
 } blest_mbfs_params;
 typedef struct blest_mbfs_stats {
     double time;
@@ -356,15 +358,50 @@ int blest_mbfs(blest_graph* g, const uint32_t* sources, uint32_t k, uint32_t* le
 int blest_mbfs_ws(blest_workspace* ws, const uint32_t* sources, uint32_t k, uint32_t* levels_out, int out_mem,
                   const blest_mbfs_params* params, void* stream, blest_mbfs_stats* stats);
 
-/* Many graphs, many sources, one persistent launch. */
+/* Many graphs, many sources, one persistent launch. The items' graphs are
+ * joined on the device into one block-diagonal graph (each graph's vertices
+ * at an offset aligned to 32); source slot j of a pass holds the j-th source
+ * of every graph at once, since their vertex sets never meet. Levels equal
+ * those of independent single-source runs on each graph. */
 typedef struct blest_mbfs_item {
     blest_graph* graph;
-    const uint32_t* sources;  /* host array, k entries */
+    const uint32_t* sources;  /* host array, k entries (local vertex ids) */
     uint32_t k;
     uint32_t* levels_out;     /* k * n, source-major; host or device per out_mem */
 } blest_mbfs_item;
+/* One-shot: builds a plan (below), runs it once, copies host outputs,
+ * destroys it. Repeated batches over the same graphs should keep a plan. */
 int blest_mbfs_batch(const blest_mbfs_item* items, uint32_t count, int out_mem, const blest_mbfs_params* params,
                      void* stream, blest_mbfs_stats* stats);
+
+/* A resident multi-graph MBFS: the joined graph, its workspace and the
+ * run (counter reset + cooperative launch + status copy) captured once
+ * into a CUDA graph that every blest_mbfs_plan_run replays. Every item's
+ * levels_out must be device memory and stays bound to the plan. */
+typedef struct blest_mbfs_plan blest_mbfs_plan;
+typedef struct blest_mbfs_plan_info {
+    uint32_t items;
+    uint32_t n;                   /* vertices of the joined graph (with alignment padding) */
+    uint64_t nnz;
+    uint64_t no_slices;
+    uint32_t groups;              /* passes: ceil(max k / group_width) */
+    uint32_t group_width;
+    int grid_blocks;
+    int captured;                 /* 1 = replayed from a CUDA graph */
+    uint64_t device_bytes;        /* joined graph + workspace + plan tables */
+} blest_mbfs_plan_info;
+int blest_mbfs_plan_create(const blest_mbfs_item* items, uint32_t count, const blest_mbfs_params* params,
+                           void* stream, blest_mbfs_plan** out);
+/* Replace item i's sources (same k); takes effect at the next run. */
+int blest_mbfs_plan_set_sources(blest_mbfs_plan* plan, uint32_t item, const uint32_t* sources);
+/* Replay the run on the plan's stream and wait; stats->time = device time. */
+int blest_mbfs_plan_run(blest_mbfs_plan* plan, blest_mbfs_stats* stats);
+/* Replay without waiting (the caller orders later work on the plan's
+ * stream); blest_mbfs_plan_sync waits and reports the run's status. */
+int blest_mbfs_plan_launch(blest_mbfs_plan* plan);
+int blest_mbfs_plan_sync(blest_mbfs_plan* plan, blest_mbfs_stats* stats);
+int blest_mbfs_plan_info_get(const blest_mbfs_plan* plan, blest_mbfs_plan_info* out);
+int blest_mbfs_plan_destroy(blest_mbfs_plan* plan);
 
 /* ======================================================================= */
 /*  Query server (continuous batching; no counterpart in the reference)     */
