@@ -104,7 +104,8 @@ class DeviceGraphView(C.Structure):
 
 
 class MbfsParams(C.Structure):
-    _fields_ = [("group_width", u32), ("blocks_per_sm", i32), ("threads_per_block", i32), ("pull_fraction", f64)]
+    _fields_ = [("group_width", u32), ("blocks_per_sm", i32), ("threads_per_block", i32), ("pull_fraction", f64),
+                ("trace", i32)]
 
 
 class MbfsStats(C.Structure):

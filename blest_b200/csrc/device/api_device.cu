@@ -282,6 +282,16 @@ int blest_graph_create(const blest_bvss_view* bvss, const blest_csr_view* csr, b
                 if (csr->row_ptrs[u + 1] > csr->row_ptrs[u]) hasIn[u >> 5] |= 1u << (u & 31);
             d.has_in = blest::upload(g, hasIn.data(), hasIn.size());
         }
+        {
+            std::vector<uint4> chunks;
+            const uint32_t* rp = csr->row_ptrs;
+            for (uint32_t u = 0; u < csr->n; ++u)
+                if (rp[u + 1] - rp[u] > blest::dev::kPullChunk)
+                    for (uint32_t e = rp[u]; e < rp[u + 1]; e += blest::dev::kPullChunk)
+                        chunks.push_back(make_uint4(u, e, std::min(e + blest::dev::kPullChunk, rp[u + 1]), 0u));
+            d.no_pull_chunks = (uint32_t)chunks.size();
+            d.pull_chunks = blest::upload(g, chunks.data(), chunks.size());
+        }
         g->undirected_edges = csr->nnz / 2;
         BLEST_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
         g->owns_stream = true;
@@ -414,7 +424,9 @@ int blest_workspace_trace(blest_workspace* ws, blest_level_trace* out, uint32_t 
     return guarded([&] {
         blest::require(ws && out && count, "null argument");
         BLEST_CUDA(cudaSetDevice(ws->g->device));
-        const uint32_t levels = ws->w.host_counters->levels + 1;  // + end record
+        // BFS: one record per level + the end record; MBFS counts its own
+        const uint32_t its = ws->w.host_counters->iterations;
+        const uint32_t levels = its ? its : ws->w.host_counters->levels + 1;
         const uint32_t k = std::min<uint32_t>(std::min<uint32_t>(levels, max), BLEST_TRACE_CAPACITY);
         BLEST_CUDA(cudaMemcpy(out, ws->w.trace, sizeof(blest_level_trace) * k, cudaMemcpyDeviceToHost));
         *count = k;

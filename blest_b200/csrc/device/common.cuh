@@ -39,7 +39,15 @@ struct DevGraph {
     const uint32_t* csr_ptrs;   // n + 1 (in-neighbours)
     const uint32_t* csr_ids;    // nnz
     const uint32_t* has_in;     // ceil(n/32) words: bit v = v has an in-neighbour (may be null)
+    // In-lists longer than kPullChunk cut into pieces of at most kPullChunk
+    // edges: {vertex, first edge, end edge, 0}, by vertex (multi-source pull).
+    const uint4* pull_chunks;
+    uint32_t no_pull_chunks;
 };
+
+// Longest in-list one lane scans whole in the multi-source pull; longer
+// lists are scanned as pieces of this many edges.
+constexpr uint32_t kPullChunk = 64;
 
 // Bit 63 of the barrier's arrival counter: some block recorded an error.
 constexpr unsigned long long kArriveError = 1ull << 63;

@@ -42,6 +42,8 @@ struct MbfsPart {
     uint32_t n;
     uint32_t k;
     uint32_t src_base;
+    uint32_t cbase;   // its first long-list piece (DevGraph::pull_chunks)
+    uint32_t ccount;  // its long-list pieces
     uint32_t* levels;
 };
 
@@ -64,6 +66,8 @@ struct MbfsArgs {
     const uint32_t* word_part;
     MbfsPart part0;
     const uint32_t* sources;   // local source ids, per part from src_base
+    uint32_t* part_nf;         // 2 slots x nparts: vertices found per part at the last two levels
+    blest_level_trace* trace;  // optional: one record per level of every group
     uint32_t groups;           // ceil(max k / group_width)
     uint32_t group_width;      // sources per group (32 * WORDS)
     float pull_fraction;       // pull when frontier vertices > n * pull_fraction
@@ -76,6 +80,8 @@ __device__ __forceinline__ MbfsPart load_part(const MbfsArgs& a, uint32_t p) {
     P.n = __ldg(&a.parts[p].n);
     P.k = __ldg(&a.parts[p].k);
     P.src_base = __ldg(&a.parts[p].src_base);
+    P.cbase = __ldg(&a.parts[p].cbase);
+    P.ccount = __ldg(&a.parts[p].ccount);
     P.levels = a.parts[p].levels;
     return P;
 }
@@ -87,6 +93,81 @@ __device__ __forceinline__ uint32_t part_of_word(const MbfsArgs& a, uint32_t wi)
 // Sources of part P in the group starting at s0 (0 when it has none left).
 __device__ __forceinline__ uint32_t group_rows(const MbfsPart& P, uint32_t s0, uint32_t width) {
     return P.k > s0 ? min(width, P.k - s0) : 0u;
+}
+
+// Calls body(p, P, word) for every 32-vertex word of every part p with
+// pred(p, P), spreading the words of all selected parts evenly over the
+// warps (warp-uniform calls). Each warp scans the part table 32 parts at a
+// time; the words of the selected parts form one flat range that warp w
+// walks from index w in steps of nwarps.
+template <class Pred, class Body>
+__device__ __forceinline__ void for_each_part_word(const MbfsArgs& a, uint32_t warp, uint32_t nwarps, Pred pred,
+                                                   Body body) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t base = 0;
+    for (uint32_t p0 = 0; p0 < a.nparts; p0 += 32) {
+        const uint32_t p = p0 + lane;
+        MbfsPart P{};
+        bool sel = false;
+        if (p < a.nparts) {
+            P = load_part(a, p);
+            sel = P.n > 0 && pred(p, P);
+        }
+        uint32_t m = __ballot_sync(0xFFFFFFFFu, sel);
+        while (m) {
+            const uint32_t ln = __ffs(m) - 1;
+            m &= m - 1;
+            const MbfsPart Q = load_part(a, p0 + ln);
+            const uint32_t words = (Q.n + 31) / 32;
+            for (uint32_t i = base + (warp + nwarps - base % nwarps) % nwarps; i < base + words; i += nwarps)
+                body(p0 + ln, Q, Q.off / 32 + (i - base));
+            base += words;
+        }
+    }
+}
+
+// Calls body(p, P, i_begin, i_end) so that the long-list pieces of all
+// parts with pred(p, P), as one flat range, are split into equal contiguous
+// shares, one per warp (warp-uniform calls; indices into pull_chunks).
+template <class Pred, class Body>
+__device__ __forceinline__ void for_each_part_chunks(const MbfsArgs& a, uint32_t warp, uint32_t nwarps, Pred pred,
+                                                     Body body) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint64_t total = 0;
+    for (uint32_t p0 = 0; p0 < a.nparts; p0 += 32) {
+        const uint32_t p = p0 + lane;
+        uint32_t cc = 0;
+        if (p < a.nparts) {
+            const MbfsPart P = load_part(a, p);
+            if (P.ccount && pred(p, P)) cc = P.ccount;
+        }
+        total += __reduce_add_sync(0xFFFFFFFFu, cc);
+    }
+    const uint64_t lo = total * warp / nwarps, hi = total * (warp + 1) / nwarps;
+    if (lo >= hi) return;
+    uint64_t base = 0;
+    for (uint32_t p0 = 0; p0 < a.nparts && base < hi; p0 += 32) {
+        const uint32_t p = p0 + lane;
+        bool sel = false;
+        uint32_t cc = 0;
+        if (p < a.nparts) {
+            const MbfsPart P = load_part(a, p);
+            sel = P.ccount && pred(p, P);
+            cc = P.ccount;
+        }
+        uint32_t m = __ballot_sync(0xFFFFFFFFu, sel);
+        while (m && base < hi) {
+            const uint32_t ln = __ffs(m) - 1;
+            m &= m - 1;
+            const uint64_t c = __shfl_sync(0xFFFFFFFFu, cc, ln);
+            const uint64_t s = max(lo, base), t = min(hi, base + c);
+            if (s < t) {
+                const MbfsPart Q = load_part(a, p0 + ln);
+                body(p0 + ln, Q, Q.cbase + (uint32_t)(s - base), Q.cbase + (uint32_t)(t - base));
+            }
+            base += c;
+        }
+    }
 }
 
 template <int WORDS>
@@ -129,6 +210,36 @@ __device__ __forceinline__ void store_bits(uint32_t* a, uint32_t v, const Bits<W
     }
 }
 
+// OR of the frontier bits of in-neighbours csr_ids[q, qe) into acc, limited
+// to `need`; four neighbours' loads in flight at a time; stops once acc
+// covers need.
+template <int WORDS>
+__device__ __forceinline__ void scan_in_list(const MbfsArgs& a, uint32_t q, uint32_t qe, const uint32_t (&need)[WORDS],
+                                             uint32_t (&acc)[WORDS]) {
+    for (; q < qe; q += 4) {
+        uint32_t u[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) u[j] = q + j < qe ? __ldg(&a.g.csr_ids[q + j]) : 0xFFFFFFFFu;
+        Bits<WORDS> f[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (u[j] != 0xFFFFFFFFu) {
+                f[j] = load_bits<WORDS>(a.frontier, u[j]);
+            } else {
+#pragma unroll
+                for (int w = 0; w < WORDS; ++w) f[j].w[w] = 0u;
+            }
+        }
+        bool covered = true;
+#pragma unroll
+        for (int w = 0; w < WORDS; ++w) {
+            acc[w] |= (f[0].w[w] | f[1].w[w] | f[2].w[w] | f[3].w[w]) & need[w];
+            covered &= acc[w] == need[w];
+        }
+        if (covered) break;
+    }
+}
+
 template <int WORDS>
 __global__ void __launch_bounds__(512, 2) mbfs_persistent_kernel(MbfsArgs a) {
     const uint32_t lane = threadIdx.x & 31;
@@ -160,6 +271,7 @@ __global__ void __launch_bounds__(512, 2) mbfs_persistent_kernel(MbfsArgs a) {
             c->aux[0] = c->aux[1] = 0;  // push queue counters (2 slots)
             c->aux[4] = c->aux[5] = 0;  // new-frontier vertex counts (2 slots)
         }
+        for (uint32_t i = tid; i < 2 * a.nparts; i += nth) a.part_nf[i] = 0u;
         if (!barrier()) return;
         // ---- seeds: pair t = (part t / width, slot t % width); the sources'
         // rsets are queued in slot 0 (duplicates are harmless)
@@ -181,6 +293,7 @@ __global__ void __launch_bounds__(512, 2) mbfs_persistent_kernel(MbfsArgs a) {
                             atomicOr(&a.visited[v * WORDS + (b >> 5)], 1u << (b & 31));
                             atomicOr(&a.frontier[v * WORDS + (b >> 5)], 1u << (b & 31));
                             P.levels[(uint64_t)(s0 + b) * P.n + src] = 0u;
+                            atomicAdd(&a.part_nf[p], 1u);  // level-0 slot
                             ++seeded;
                             r = v >> 3;
                             const uint32_t tl = __ldg(&g.rset_tile[r + 1]) - __ldg(&g.rset_tile[r]);
@@ -213,116 +326,206 @@ __global__ void __launch_bounds__(512, 2) mbfs_persistent_kernel(MbfsArgs a) {
         if (!barrier()) return;
 
         for (uint32_t level = 1;; ++level) {
-            const uint32_t slot = (level - 1) & 1;  // queue/count produced by the previous sweep
+            const uint32_t slot = (level - 1) & 1;  // queue/counts produced by the previous sweep
             const uint64_t nf = ld_relaxed64(&c->aux[4 + slot]);
+            if (a.trace && tid == 0 && c->iterations < BLEST_TRACE_CAPACITY) {
+                // direction summary: 1 push, 2 pull, 3 both (several graphs)
+                uint32_t dirs = 0;
+                for (uint32_t p = 0; p < a.nparts && dirs != 3; ++p) {
+                    const MbfsPart P = load_part(a, p);
+                    const uint32_t x = __ldcg(&a.part_nf[slot * a.nparts + p]);
+                    if (x) dirs |= (double)x > (double)P.n * a.pull_fraction ? 2u : 1u;
+                }
+                blest_level_trace& t = a.trace[c->iterations++];
+                t.start_ns = global_ns();
+                t.level = nf ? level : 0;
+                t.direction = dirs;
+                t.frontier = nf;
+                t.work_units = ld_relaxed64(&c->aux[slot]) & kQUnitMask;
+                t.longest_scan = grp;
+            }
             if (nf == 0) break;
             if (level > n + 1) {
                 set_error(c, BLEST_ERR_LEVEL_CAP);
                 return;
             }
-            const bool pull = (double)nf > (double)n * a.pull_fraction;
             if (tid == 0) {
                 c->aux[slot ^ 1] = 0;      // queue slot the coming sweep fills
                 c->aux[4 + (slot ^ 1)] = 0;
             }
-            // ---- expand
-            if (pull) {
-                for (uint32_t v = tid; v < n; v += nth) {
-                    uint32_t valid[WORDS];
-                    rows_mask<WORDS>(group_rows(load_part(a, part_of_word(a, v >> 5)), s0, a.group_width), valid);
+            for (uint32_t p = tid; p < a.nparts; p += nth) a.part_nf[(slot ^ 1) * a.nparts + p] = 0u;
+            // Per graph: active = it found vertices at level L-1; it pulls
+            // when that frontier holds more than n * pull_fraction vertices.
+            const uint32_t* nfp = a.part_nf + slot * a.nparts;
+            auto pulls = [&](uint32_t p, const MbfsPart& P) {
+                const uint32_t x = __ldcg(&nfp[p]);
+                return x > 0 && (double)x > (double)P.n * a.pull_fraction;
+            };
+            // ---- expand, pulling graphs. In-lists of at most kPullChunk
+            // edges: one lane per vertex, scanned whole (4 loads in flight)
+            // until the bits v still needs are covered; longer lists: one
+            // lane per kPullChunk-edge piece from the static piece table,
+            // merged into next[v] with atomicOr. No lane scans more than
+            // kPullChunk edges, so no list sets the level's time.
+            for_each_part_word(a, warp, nwarps, pulls, [&](uint32_t p, const MbfsPart& P, uint32_t wi) {
+                const uint32_t v = wi * 32 + lane;
+                if (v - P.off >= P.n) return;
+                const uint32_t pb = __ldg(&g.csr_ptrs[v]), pe = __ldg(&g.csr_ptrs[v + 1]);
+                if (pe - pb > kPullChunk || pe == pb) return;
+                uint32_t valid[WORDS];
+                rows_mask<WORDS>(group_rows(P, s0, a.group_width), valid);
+                const Bits<WORDS> vis = load_bits<WORDS>(a.visited, v);
+                uint32_t need[WORDS], acc[WORDS];
+                bool any = false;
+#pragma unroll
+                for (int w = 0; w < WORDS; ++w) {
+                    need[w] = ~vis.w[w] & valid[w];
+                    acc[w] = 0u;
+                    any |= need[w] != 0;
+                }
+                if (!any) return;
+                scan_in_list<WORDS>(a, pb, pe, need, acc);
+                bool got = false;
+                Bits<WORDS> out;
+#pragma unroll
+                for (int w = 0; w < WORDS; ++w) {
+                    out.w[w] = acc[w];
+                    got |= acc[w] != 0;
+                }
+                if (got) store_bits<WORDS>(a.next, v, out);
+            });
+            for_each_part_chunks(a, warp, nwarps, pulls, [&](uint32_t p, const MbfsPart& P, uint32_t cb, uint32_t ce) {
+                uint32_t valid[WORDS];
+                rows_mask<WORDS>(group_rows(P, s0, a.group_width), valid);
+                for (uint32_t i = cb + lane; i < ce; i += 32) {
+                    const uint4 piece = __ldg(&g.pull_chunks[i]);
+                    const uint32_t v = piece.x;
                     const Bits<WORDS> vis = load_bits<WORDS>(a.visited, v);
-                    Bits<WORDS> need, acc;
+                    uint32_t need[WORDS], acc[WORDS];
                     bool any = false;
 #pragma unroll
                     for (int w = 0; w < WORDS; ++w) {
-                        need.w[w] = ~vis.w[w] & valid[w];
-                        acc.w[w] = 0u;
-                        any |= need.w[w] != 0;
+                        need[w] = ~vis.w[w] & valid[w];
+                        acc[w] = 0u;
+                        any |= need[w] != 0;
                     }
                     if (!any) continue;
-                    const uint32_t pb = __ldg(&g.csr_ptrs[v]), pe = __ldg(&g.csr_ptrs[v + 1]);
-                    for (uint32_t p = pb; p < pe; p += 2) {
-                        const uint32_t u0 = __ldg(&g.csr_ids[p]);
-                        const uint32_t u1 = p + 1 < pe ? __ldg(&g.csr_ids[p + 1]) : u0;
-                        const Bits<WORDS> f0 = load_bits<WORDS>(a.frontier, u0);
-                        const Bits<WORDS> f1 = load_bits<WORDS>(a.frontier, u1);
-                        bool covered = true;
+                    scan_in_list<WORDS>(a, piece.y, piece.z, need, acc);
 #pragma unroll
-                        for (int w = 0; w < WORDS; ++w) {
-                            acc.w[w] |= (f0.w[w] | f1.w[w]) & need.w[w];
-                            covered &= acc.w[w] == need.w[w];
-                        }
-                        if (covered) break;
-                    }
-                    bool got = false;
-#pragma unroll
-                    for (int w = 0; w < WORDS; ++w) got |= acc.w[w] != 0;
-                    if (got) store_bits<WORDS>(a.next, v, acc);
+                    for (int w = 0; w < WORDS; ++w)
+                        if (acc[w]) atomicOr(&a.next[v * WORDS + w], acc[w]);
                 }
-            } else {
+            });
+            // ---- expand, pushing graphs: the queued rsets' tiles. Each warp
+            // takes a contiguous range of 32-tile chunks, finds the owner
+            // entry of its first chunk once and walks the queue forward;
+            // entries of pulling graphs are skipped whole.
+            const bool single_pulls = !a.parts && pulls(0, a.part0);
+            if (!single_pulls) {
                 const uint64_t qc = ld_relaxed64(&c->aux[slot]);
                 const uint32_t E = (uint32_t)(qc >> kQShift), U = (uint32_t)(qc & kQUnitMask);
                 const uint32_t* qr = a.q_rset + slot * a.qreg;
                 const uint32_t* qo = a.q_off + slot * a.qreg;
-                for (uint32_t ch = warp; ch < U; ch += nwarps) {
-                    // owner entry of chunk ch (binary search, warp-uniform)
-                    uint32_t lo = 0, hi = E;
-                    while (hi - lo > 1) {
-                        const uint32_t mid = (lo + hi) / 2;
-                        if (__ldcg(&qo[mid]) <= ch) lo = mid;
-                        else hi = mid;
+                const uint32_t per = (U + nwarps - 1) / nwarps;
+                uint32_t ch = warp * per;
+                const uint32_t cend = min(U, ch + per);
+                if (ch < cend) {
+                    uint32_t e;
+                    {
+                        // largest entry with q_off <= ch: warp-wide sampled search
+                        uint32_t lo = 0, hi = E;
+                        while (hi - lo > 32) {
+                            const uint32_t step = (hi - lo + 31) / 32;
+                            const uint32_t idx = lo + lane * step;
+                            const bool ok = idx < hi && __ldcg(&qo[idx]) <= ch;
+                            const uint32_t cnt = __popc(__ballot_sync(0xFFFFFFFFu, ok));
+                            const uint32_t nlo = lo + (cnt - 1) * step;
+                            hi = min(hi, nlo + step);
+                            lo = nlo;
+                        }
+                        const uint32_t idx = lo + lane;
+                        const bool ok = idx < hi && __ldcg(&qo[idx]) <= ch;
+                        e = lo + __popc(__ballot_sync(0xFFFFFFFFu, ok)) - 1;
                     }
-                    const uint32_t r = __ldcg(&qr[lo]);
-                    const uint32_t off = __ldcg(&qo[lo]);
-                    const uint32_t t0 = __ldg(&g.rset_tile[r]), t1 = __ldg(&g.rset_tile[r + 1]);
-                    const uint32_t tile = t0 + (ch - off) * 32 + lane;
-                    // frontier words of the rset's 8 columns, lane k holds column k
-                    Bits<WORDS> fc;
-#pragma unroll
-                    for (int w = 0; w < WORDS; ++w) fc.w[w] = 0u;
-                    if (lane < 8 && r * 8 + lane < n) fc = load_bits<WORDS>(a.frontier, r * 8 + lane);
-                    uint4 rows = make_uint4(0, 0, 0, 0);
-                    uint32_t mask = 0;
-                    if (tile < t1) {
-                        rows = ld_stream(&g.row4[tile]);
-                        mask = ld_stream(&g.masks[tile]);
-                    }
-                    Bits<WORDS> col[8];
-#pragma unroll
-                    for (int k = 0; k < 8; ++k)
-#pragma unroll
-                        for (int w = 0; w < WORDS; ++w) col[k].w[w] = __shfl_sync(0xFFFFFFFFu, fc.w[w], k);
-                    const uint32_t rk[4] = {rows.x, rows.y, rows.z, rows.w};
-#pragma unroll
-                    for (int s = 0; s < 4; ++s) {
-                        const uint32_t mb = (mask >> (8 * s)) & 0xFFu;
-                        if (!mb) continue;
-                        const uint32_t row = rk[s];
-                        if (row >= n) {
-                            set_error(c, BLEST_ERR_DEVICE_INDEX);
+                    uint32_t r = 0, off = 0, eend = 0;
+                    bool skip = false;
+                    uint32_t lastp = 0xFFFFFFFFu;
+                    bool lastpull = false;
+                    auto enter = [&](uint32_t ei) {
+                        r = __ldcg(&qr[ei]);
+                        off = __ldcg(&qo[ei]);
+                        eend = ei + 1 < E ? __ldcg(&qo[ei + 1]) : U;
+                        const uint32_t p = a.parts ? part_of_word(a, r >> 2) : 0u;
+                        if (p != lastp) {
+                            lastp = p;
+                            lastpull = a.parts ? pulls(p, load_part(a, p)) : false;
+                        }
+                        skip = lastpull;
+                    };
+                    enter(e);
+                    while (ch < cend) {
+                        if (ch >= eend) {
+                            enter(++e);
                             continue;
                         }
-                        Bits<WORDS> acc;
+                        if (skip) {
+                            ch = eend;  // next entry
+                            continue;
+                        }
+                        const uint32_t t0 = __ldg(&g.rset_tile[r]), t1 = __ldg(&g.rset_tile[r + 1]);
+                        const uint32_t tile = t0 + (ch - off) * 32 + lane;
+                        // frontier words of the rset's 8 columns, lane k holds column k
+                        Bits<WORDS> fc;
 #pragma unroll
-                        for (int w = 0; w < WORDS; ++w) acc.w[w] = 0u;
+                        for (int w = 0; w < WORDS; ++w) fc.w[w] = 0u;
+                        if (lane < 8 && r * 8 + lane < n) fc = load_bits<WORDS>(a.frontier, r * 8 + lane);
+                        uint4 rows = make_uint4(0, 0, 0, 0);
+                        uint32_t mask = 0;
+                        if (tile < t1) {
+                            rows = ld_stream(&g.row4[tile]);
+                            mask = ld_stream(&g.masks[tile]);
+                        }
+                        Bits<WORDS> col[8];
 #pragma unroll
                         for (int k = 0; k < 8; ++k)
-                            if ((mb >> k) & 1u)
 #pragma unroll
-                                for (int w = 0; w < WORDS; ++w) acc.w[w] |= col[k].w[w];
-                        const Bits<WORDS> vis = load_bits<WORDS>(a.visited, row);
+                            for (int w = 0; w < WORDS; ++w) col[k].w[w] = __shfl_sync(0xFFFFFFFFu, fc.w[w], k);
+                        const uint32_t rk[4] = {rows.x, rows.y, rows.z, rows.w};
 #pragma unroll
-                        for (int w = 0; w < WORDS; ++w) {
-                            const uint32_t add = acc.w[w] & ~vis.w[w];
-                            if (add) atomicOr(&a.next[row * WORDS + w], add);
+                        for (int s = 0; s < 4; ++s) {
+                            const uint32_t mb = (mask >> (8 * s)) & 0xFFu;
+                            if (!mb) continue;
+                            const uint32_t row = rk[s];
+                            if (row >= n) {
+                                set_error(c, BLEST_ERR_DEVICE_INDEX);
+                                continue;
+                            }
+                            Bits<WORDS> acc;
+#pragma unroll
+                            for (int w = 0; w < WORDS; ++w) acc.w[w] = 0u;
+#pragma unroll
+                            for (int k = 0; k < 8; ++k)
+                                if ((mb >> k) & 1u)
+#pragma unroll
+                                    for (int w = 0; w < WORDS; ++w) acc.w[w] |= col[k].w[w];
+                            const Bits<WORDS> vis = load_bits<WORDS>(a.visited, row);
+#pragma unroll
+                            for (int w = 0; w < WORDS; ++w) {
+                                const uint32_t add = acc.w[w] & ~vis.w[w];
+                                if (add) atomicOr(&a.next[row * WORDS + w], add);
+                            }
                         }
+                        ++ch;
                     }
                 }
             }
             if (!barrier()) return;
-            // ---- sweep: whole warps over 32 consecutive vertices
+            // ---- sweep over the active graphs' words (an inactive graph has
+            // an empty frontier and received no next bits)
             uint32_t cnt = 0;
-            for (uint32_t wi = warp; wi < Wn; wi += nwarps) {
+            uint32_t* nfn = a.part_nf + (slot ^ 1) * a.nparts;
+            auto active = [&](uint32_t p, const MbfsPart&) { return __ldcg(&nfp[p]) > 0; };
+            for_each_part_word(a, warp, nwarps, active, [&](uint32_t p, const MbfsPart& P, uint32_t wi) {
                 const uint32_t v = wi * 32 + lane;
                 Bits<WORDS> nw;
                 bool any = false;
@@ -356,11 +559,11 @@ __global__ void __launch_bounds__(512, 2) mbfs_persistent_kernel(MbfsArgs a) {
                     for (int w = 0; w < WORDS; ++w) nw.w[w] = 0u;
                 }
                 const uint32_t anyMask = __ballot_sync(0xFFFFFFFFu, any);
-                if (!anyMask) continue;
+                if (!anyMask) return;
                 cnt += any ? 1u : 0u;
+                if (lane == 0) atomicAdd(&nfn[p], (uint32_t)__popc(anyMask));
                 // levels of the new (source, vertex) pairs, one source row at
-                // a time (new bits only arise in real vertices of the part)
-                const MbfsPart P = load_part(a, part_of_word(a, wi));
+                // a time (new bits only arise in real vertices of the graph)
                 const uint32_t lv = v - P.off;
 #pragma unroll
                 for (int w = 0; w < WORDS; ++w) {
@@ -397,7 +600,7 @@ __global__ void __launch_bounds__(512, 2) mbfs_persistent_kernel(MbfsArgs a) {
                         }
                     }
                 }
-            }
+            });
             const uint64_t wc = warp_sum64(cnt);
             if (lane == 0 && wc) atomicAdd(&c->aux[4 + (slot ^ 1)], (unsigned long long)wc);
             if (tid == 0) c->levels = max(c->levels, level);
@@ -415,7 +618,8 @@ struct MbfsScratch {
     uint32_t* levels = nullptr; // staging for host output
     uint32_t* sources = nullptr;
     uint32_t* queue = nullptr;  // rset queue: 2 slots of entries + 2 slots of offsets
-    size_t state_words = 0, levels_words = 0, sources_cap = 0, queue_words = 0;
+    uint32_t* part_nf = nullptr;  // per-graph frontier counts, 2 slots
+    size_t state_words = 0, levels_words = 0, sources_cap = 0, queue_words = 0, part_nf_cap = 0;
 };
 
 // Entries one queue slot needs: a sweep queues each rset at most once; the
@@ -443,7 +647,7 @@ struct MbfsLaunch {
 
 template <int WORDS>
 void prepare_words(const blest_graph* g, blest::Workspace& w, MbfsScratch& sc, const blest_mbfs_params& p,
-                   uint64_t seeds, MbfsLaunch& L) {
+                   uint64_t seeds, uint32_t nparts, MbfsLaunch& L) {
     const uint32_t n = g->d.n;
     ensure(sc.state, sc.state_words, 3ull * n * WORDS);
     dev::MbfsArgs& a = L.a;
@@ -455,6 +659,9 @@ void prepare_words(const blest_graph* g, blest::Workspace& w, MbfsScratch& sc, c
     ensure(sc.queue, sc.queue_words, 4ull * a.qreg);
     a.q_rset = sc.queue;
     a.q_off = sc.queue + 2ull * a.qreg;
+    ensure(sc.part_nf, sc.part_nf_cap, 2ull * nparts);
+    a.part_nf = sc.part_nf;
+    a.trace = p.trace ? w.trace : nullptr;
     a.ctr = w.counters;
     a.group_width = 32 * WORDS;
     a.pull_fraction = p.pull_fraction > 0 ? (float)p.pull_fraction : 1.0f / 64.0f;
@@ -472,12 +679,12 @@ void prepare_words(const blest_graph* g, blest::Workspace& w, MbfsScratch& sc, c
 // `seeds`: the most sources one group seeds (sum over graphs of their
 // sources in a group), which sizes the rset queue.
 MbfsLaunch prepare_mbfs(const blest_graph* g, blest::Workspace& w, MbfsScratch& sc, const blest_mbfs_params& p,
-                        uint64_t seeds) {
+                        uint64_t seeds, uint32_t nparts) {
     MbfsLaunch L;
     const uint32_t gw = p.group_width ? p.group_width : 128;
-    if (gw == 128) prepare_words<4>(g, w, sc, p, seeds, L);
-    else if (gw == 64) prepare_words<2>(g, w, sc, p, seeds, L);
-    else if (gw == 32) prepare_words<1>(g, w, sc, p, seeds, L);
+    if (gw == 128) prepare_words<4>(g, w, sc, p, seeds, nparts, L);
+    else if (gw == 64) prepare_words<2>(g, w, sc, p, seeds, nparts, L);
+    else if (gw == 32) prepare_words<1>(g, w, sc, p, seeds, nparts, L);
     else throw Error(BLEST_ERR_INVALID_ARG, "group_width must be 32, 64 or 128");
     return L;
 }
@@ -498,6 +705,7 @@ void mbfs_reserve(Workspace& w, uint32_t n, uint32_t words) {
     ensure(sc.state, sc.state_words, 3ull * n * words);
     ensure(sc.sources, sc.sources_cap, 128);
     ensure(sc.queue, sc.queue_words, 4ull * mbfs_queue_slot((n + 7) / 8, 32u * words));
+    ensure(sc.part_nf, sc.part_nf_cap, 2);
 }
 
 void mbfs_scratch_free(void* p) {
@@ -507,6 +715,7 @@ void mbfs_scratch_free(void* p) {
     cudaFree(sc->levels);
     cudaFree(sc->sources);
     cudaFree(sc->queue);
+    cudaFree(sc->part_nf);
     delete sc;
 }
 
@@ -524,7 +733,7 @@ struct JoinSeg {
     uint32_t kind;  // JoinKind
     uint32_t pad;
 };
-enum JoinKind : uint32_t { kAdd32 = 0, kAdd32KeepPad = 1, kAdd64 = 2, kFill32 = 3, kFill64 = 4 };
+enum JoinKind : uint32_t { kAdd32 = 0, kAdd32KeepPad = 1, kAdd64 = 2, kFill32 = 3, kFill64 = 4, kPiece = 5 };
 
 // blockIdx.y = segment (of this chunk of the table); the x blocks stride it.
 __global__ void join_kernel(const JoinSeg* segs) {
@@ -546,6 +755,12 @@ __global__ void join_kernel(const JoinSeg* segs) {
         case kFill32:
             static_cast<uint32_t*>(sg.dst)[i] = (uint32_t)sg.add;
             break;
+        case kPiece: {  // {vertex + add.lo, edges + add.hi}
+            const uint4 x = static_cast<const uint4*>(sg.src)[i];
+            const uint32_t av = (uint32_t)sg.add, ae = (uint32_t)(sg.add >> 32);
+            static_cast<uint4*>(sg.dst)[i] = make_uint4(x.x + av, x.y + ae, x.z + ae, 0u);
+            break;
+        }
         default:
             static_cast<uint64_t*>(sg.dst)[i] = sg.add;
             break;
@@ -573,13 +788,14 @@ T* plan_alloc(blest_graph* u, size_t count) {
 void join_graphs(const std::vector<const blest_graph*>& gs, const std::vector<uint32_t>& off, uint32_t N,
                  blest_graph* u, cudaStream_t s) {
     using dev::JoinSeg;
-    uint64_t V = 0, T = 0, E = 0;
+    uint64_t V = 0, T = 0, E = 0, C = 0;
     for (auto* g : gs) {
         V += g->d.no_virtual;
         T += g->d.no_slices / 4;
         E += g->d.nnz;
+        C += g->d.no_pull_chunks;
     }
-    if (V >= 0xFFFFFFFFull || T >= 0xFFFFFFFFull || E >= 0xFFFFFFFFull)
+    if (V >= 0xFFFFFFFFull || T >= 0xFFFFFFFFull || E >= 0xFFFFFF00ull || C >= 0xFFFFFFFFull)
         throw Error(BLEST_ERR_UNSUPPORTED, "joined graph exceeds 2^32 vertex sets, tiles or edges");
     const uint32_t R = N / 8;
     dev::DevGraph& d = u->d;
@@ -598,11 +814,12 @@ void join_graphs(const std::vector<const blest_graph*>& gs, const std::vector<ui
     uint32_t* cp = plan_alloc<uint32_t>(u, (size_t)N + 1);
     uint32_t* ci = plan_alloc<uint32_t>(u, E);
     uint32_t* hin = plan_alloc<uint32_t>(u, (size_t)N / 32 + 4);
+    uint4* pieces = plan_alloc<uint4>(u, C);
     std::vector<JoinSeg> segs;
     auto seg = [&](const void* src, void* dst, uint64_t count, uint64_t add, uint32_t kind) {
         if (count) segs.push_back(JoinSeg{src, dst, count, add, kind, 0});
     };
-    uint64_t vo = 0, to = 0, eo = 0;
+    uint64_t vo = 0, to = 0, eo = 0, co = 0;
     for (size_t i = 0; i < gs.size(); ++i) {
         const dev::DevGraph& g = gs[i]->d;
         const uint32_t o = off[i], ri = g.no_real, rpad = (o + ((g.n + 31) & ~31u)) / 8 - o / 8;
@@ -620,9 +837,11 @@ void join_graphs(const std::vector<const blest_graph*>& gs, const std::vector<ui
         seg(g.csr_ids, ci + eo, g.nnz, o, dev::kAdd32);
         if (g.has_in) seg(g.has_in, hin + o / 32, (g.n + 31) / 32, 0, dev::kAdd32);
         else seg(nullptr, hin + o / 32, (g.n + 31) / 32, 0xFFFFFFFFull, dev::kFill32);
+        seg(g.pull_chunks, pieces + co, g.no_pull_chunks, (uint64_t)o | (eo << 32), dev::kPiece);
         vo += g.no_virtual;
         to += ti;
         eo += g.nnz;
+        co += g.no_pull_chunks;
     }
     seg(nullptr, ssp + V, 1, 4 * T, dev::kFill64);
     seg(nullptr, rp + R, 1, V, dev::kFill32);
@@ -650,6 +869,8 @@ void join_graphs(const std::vector<const blest_graph*>& gs, const std::vector<ui
     d.csr_ptrs = cp;
     d.csr_ids = ci;
     d.has_in = hin;
+    d.pull_chunks = pieces;
+    d.no_pull_chunks = (uint32_t)C;
     u->undirected_edges = E / 2;
 }
 
@@ -743,11 +964,11 @@ int blest_mbfs_ws(blest_workspace* ws, const uint32_t* sources, uint32_t k, uint
             blest::ensure(sc.levels, sc.levels_words, (size_t)k * n);
             dl = sc.levels;
         }
-        blest::MbfsLaunch L = blest::prepare_mbfs(g, w, sc, p, std::min(k, gw));
+        blest::MbfsLaunch L = blest::prepare_mbfs(g, w, sc, p, std::min(k, gw), 1);
         L.a.parts = nullptr;
         L.a.nparts = 1;
         L.a.word_part = nullptr;
-        L.a.part0 = blest::dev::MbfsPart{0u, n, k, 0u, dl};
+        L.a.part0 = blest::dev::MbfsPart{0u, n, k, 0u, 0u, g->d.no_pull_chunks, dl};
         L.a.sources = sc.sources;
         L.a.groups = (k + gw - 1) / gw;
         BLEST_CUDA(cudaEventRecord(w.ev_start, s));
@@ -831,11 +1052,13 @@ int blest_mbfs_plan_create(const blest_mbfs_item* items, uint32_t count, const b
         // parts, word -> part map, sources
         std::vector<uint32_t> wordPart(N / 32);
         std::vector<uint32_t> src(std::max<uint64_t>(K, 1));
-        uint32_t base = 0;
+        uint32_t base = 0, cbase = 0;
         p->parts.resize(count);
         for (uint32_t i = 0; i < count; ++i) {
             const uint32_t n = gs[i]->d.n;
-            p->parts[i] = blest::dev::MbfsPart{off[i], n, items[i].k, base, items[i].levels_out};
+            p->parts[i] = blest::dev::MbfsPart{off[i], n, items[i].k, base, cbase, gs[i]->d.no_pull_chunks,
+                                               items[i].levels_out};
+            cbase += gs[i]->d.no_pull_chunks;
             std::fill(wordPart.begin() + off[i] / 32, wordPart.begin() + off[i] / 32 + (n + 31) / 32, i);
             std::copy(items[i].sources, items[i].sources + items[i].k, src.begin() + base);
             base += items[i].k;
@@ -850,7 +1073,7 @@ int blest_mbfs_plan_create(const blest_mbfs_item* items, uint32_t count, const b
         blest::MbfsScratch& sc = *(blest::MbfsScratch*)p->ws->w.mbfs;
         uint64_t seeds = 0;
         for (uint32_t i = 0; i < count; ++i) seeds += std::min(items[i].k, prm.group_width);
-        p->L = blest::prepare_mbfs(p->u, p->ws->w, sc, prm, seeds);
+        p->L = blest::prepare_mbfs(p->u, p->ws->w, sc, prm, seeds, count);
         p->L.a.parts = p->d_parts;
         p->L.a.nparts = count;
         p->L.a.word_part = p->d_word_part;

@@ -134,6 +134,9 @@ int run_job(blest_server* s, Lane& lane, Job& job) {
     if (s->p.dry_run) {
         for (Request* r : job.reqs)
             if (r->out) r->out[0] = (uint32_t)job.reqs.size();  // marks the batch in dry runs
+        // stands in for the device time of a job, so that requests arriving
+        // meanwhile queue up behind it as they would behind a real run
+        std::this_thread::sleep_for(std::chrono::microseconds(500));
         return BLEST_OK;
     }
     cudaSetDevice(s->device);

@@ -330,7 +330,7 @@ class Graph:
         out = []
         for i in range(cnt.value):
             r = recs[i]
-            out.append({"level": r.level, "dir": {1: "push", 2: "pull"}.get(r.direction, "end"),
+            out.append({"level": r.level, "dir": {1: "push", 2: "pull", 3: "both"}.get(r.direction, "end"),
                         "start_ns": r.start_ns, "frontier": r.frontier, "work_units": r.work_units,
                         "longest_scan": r.longest_scan})
         return out
@@ -367,11 +367,11 @@ class Graph:
         return lab, CcStats(st.time, st.no_components, st.iterations)
 
     def mbfs(self, sources, group_width: int = 128, blocks_per_sm: int = 0, threads_per_block: int = 0,
-             pull_fraction: float = 0.0):
+             pull_fraction: float = 0.0, trace: bool = False):
         """Multi-source BFS: returns (levels[k, n], MbfsStats)."""
         src = np.ascontiguousarray(sources, dtype=np.uint32)
         out = np.empty((src.size, self.n), dtype=np.uint32)
-        p = L.MbfsParams(group_width, blocks_per_sm, threads_per_block, pull_fraction)
+        p = L.MbfsParams(group_width, blocks_per_sm, threads_per_block, pull_fraction, int(trace))
         st = L.MbfsStats()
         L.call("blest_mbfs", self._h, _u32p(src), src.size, out.ctypes.data, L.MEM_HOST, C.byref(p), C.byref(st))
         return out, MbfsStats(st.time, st.groups, st.max_levels, st.reached_degree_sum)

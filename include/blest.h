@@ -275,7 +275,8 @@ int blest_bfs(blest_graph* g, uint32_t source, uint32_t* levels_out, uint32_t* p
 int blest_bfs_ws(blest_workspace* ws, uint32_t source, uint32_t* levels_out, uint32_t* parents_out, int out_mem,
                  const blest_bfs_params* params, void* stream, int async, blest_bfs_stats* stats);
 int blest_workspace_sync(blest_workspace* ws, blest_bfs_stats* stats);
-/* Level records of the last traced BFS on `ws` (at most `max`). */
+/* Level records of the last traced BFS (or multi-source BFS: one record per
+ * level of every group, direction 1 push / 2 pull / 3 both) on `ws`. */
 int blest_workspace_trace(blest_workspace* ws, blest_level_trace* out, uint32_t max, uint32_t* count);
 /* The default workspace of a graph (owned by the graph). */
 int blest_graph_default_workspace(blest_graph* g, blest_workspace** out);
@@ -345,6 +346,7 @@ typedef struct blest_mbfs_params {
     int threads_per_block;    /* 0 = 512 */
     double pull_fraction;     /* a level pulls when its frontier has more than
                                  n * pull_fraction vertices (0 = 1/64) */
+    int trace;                /* 1 = record per-level timings (blest_workspace_trace) */
 } blest_mbfs_params;
 typedef struct blest_mbfs_stats {
     double time;
