@@ -223,8 +223,9 @@ def run_mbfs(args, rank, world):
     if not args.no_autotune_mbfs:
         from blest_b200.autotune import tune_mbfs
         tuned, table = tune_mbfs(g, sources)
-        log(f"[autotune] mbfs best {tuned} ({table[0]['seconds'] * 1e3:.2f} ms; worst {table[-1]['seconds'] * 1e3:.2f})")
-        p = L.MbfsParams(tuned["group_width"], tuned["blocks_per_sm"], 0)
+        log(f"[autotune] mbfs best {tuned} ({table[0]['seconds'] * 1e6:.2f} us/source; "
+            f"worst {table[-1]['seconds'] * 1e6:.2f})")
+        p = L.MbfsParams(tuned["group_width"], tuned["blocks_per_sm"], 0, tuned.get("pull_fraction", 0.0))
     else:
         p = L.MbfsParams(args.group_width, 0, 0)
     st = L.MbfsStats()
@@ -301,6 +302,7 @@ def run_mbfs(args, rank, world):
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generator; see config)",
         "config": {"workload": args.workload, "description": desc, "n": n, "sources_per_step": k,
                    "group_width": p.group_width, "blocks_per_sm": p.blocks_per_sm or "max",
+                   "pull_fraction": p.pull_fraction or 1 / 64,
                    "autotuned": tuned is not None, "reached_edges_per_step": mr,
                    "plain_one_launch_per_source_gteps": round(plain, 3),
                    "speedup_vs_plain": round(value / world / plain, 2),

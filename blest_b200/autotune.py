@@ -26,7 +26,7 @@ BFS_SPACE = {
     "beta": [8.0, 24.0, 96.0],
     "slice_test": ["cuda_core", "mma"],
 }
-MBFS_SPACE = {"group_width": [32, 64, 128], "blocks_per_sm": [1, 2]}
+MBFS_SPACE = {"group_width": [32, 64, 128], "blocks_per_sm": [1, 2], "pull_fraction": [1 / 256, 1 / 64, 1 / 16]}
 
 
 def _key(graph: Graph) -> str:
@@ -90,8 +90,11 @@ def tune_bfs(graph: Graph, sources, space: dict | None = None, cache: str | None
     return bfs_params(**best), table
 
 
-def tune_mbfs(graph: Graph, sources, space: dict | None = None, cache: str | None = None) -> tuple[dict, list]:
-    """Best multi-source parameters for `graph` on `sources`; returns (params, table)."""
+def tune_mbfs(graph: Graph, sources, space: dict | None = None, cache: str | None = None,
+              max_sources: int = 256) -> tuple[dict, list]:
+    """Best multi-source parameters for `graph` on (a sample of at most
+    max_sources of) `sources`; returns (params, table). seconds are per
+    source."""
     import ctypes as C
 
     import torch
@@ -100,17 +103,19 @@ def tune_mbfs(graph: Graph, sources, space: dict | None = None, cache: str | Non
     if hit:
         return hit["params"], hit["table"]
     space = space or MBFS_SPACE
-    src = np.ascontiguousarray(sources, dtype=np.uint32)
+    src = np.ascontiguousarray(np.asarray(sources)[:max_sources], dtype=np.uint32)
     out = torch.empty((src.size, graph.n), dtype=torch.int32, device="cuda")
     table = []
-    for gw, bps in itertools.product(space["group_width"], space["blocks_per_sm"]):
-        p = L.MbfsParams(gw, bps, 0)
+    for gw, bps, pf in itertools.product(space["group_width"], space["blocks_per_sm"],
+                                         space.get("pull_fraction", [0.0])):
+        p = L.MbfsParams(gw, bps, 0, pf)
         st = L.MbfsStats()
         call = lambda: L.call("blest_mbfs", graph._h, src.ctypes.data_as(L.P(L.u32)), src.size,  # noqa: E731
                               out.data_ptr(), L.MEM_DEVICE, C.byref(p), C.byref(st))
         call()
         call()
-        table.append({"params": {"group_width": gw, "blocks_per_sm": bps}, "seconds": st.time})
+        table.append({"params": {"group_width": gw, "blocks_per_sm": bps, "pull_fraction": pf},
+                      "seconds": st.time / src.size})
     del out
     table.sort(key=lambda r: r["seconds"])
     _store(cache, key, "mbfs", {"params": table[0]["params"], "table": table, "when": time.time()})

@@ -11,7 +11,9 @@
 // queued with running tile offsets (even split of tiles over warps), the
 // active bitmaps are triple-buffered and cleared through the queue two
 // iterations back, and each iteration ends in one bounded grid barrier
-// (the reference sweeps all n/32 words and syncs three times).
+// (the reference sweeps all n/32 words and syncs three times). A warp
+// works on 32 tiles of ONE rset at a time, so the rset's 8 column labels
+// are read once (8 lanes, one sector) and shared by shuffle.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -42,8 +44,9 @@ __device__ __forceinline__ uint32_t* active_buf(const CcArgs& a, uint32_t it) {
     return m == 0 ? a.active0 : (m == 1 ? a.active1 : a.active2);
 }
 
+// Queue units of an rset: its 32-tile chunks.
 __device__ __forceinline__ uint32_t tiles_of(const DevGraph& g, uint32_t r) {
-    return __ldg(&g.rset_tile[r + 1]) - __ldg(&g.rset_tile[r]);
+    return (__ldg(&g.rset_tile[r + 1]) - __ldg(&g.rset_tile[r]) + 31) / 32;
 }
 
 struct CcEnqueue {
@@ -161,53 +164,48 @@ __global__ void __launch_bounds__(512) cc_persistent_kernel(CcArgs a) {
         q.cnt = 0;
         q.units = 0;
         uint32_t changes = 0;
-        const uint32_t steps = (Uin + 31) / 32;
-        const uint32_t k = (steps + nwarps - 1) / nwarps;
+        const uint32_t k = (Uin + nwarps - 1) / nwarps;  // chunks per warp
         uint32_t s = warp * k;
-        const uint32_t send = min(steps, s + k);
+        const uint32_t send = min(Uin, s + k);
         if (s < send) {
-            uint32_t owner = cc_find_owner(qo, 0, Ein, s * 32);
+            uint32_t owner = cc_find_owner(qo, 0, Ein, s);
             for (; s < send; ++s) {
-                const uint32_t pos = s * 32 + lane;
+                // entries owner..owner+31 cover chunk s
                 const uint32_t ei = owner + lane;
                 const bool in = ei < Ein;
                 const uint32_t eoff = in ? __ldcg(&qo[ei]) : 0xFFFFFFFFu;
                 const uint32_t ers = in ? __ldcg(&qr[ei]) : 0u;
-                uint32_t lo = 0;
+                const uint32_t my = __popc(__ballot_sync(0xFFFFFFFFu, eoff <= s)) - 1;
+                const uint32_t r = __shfl_sync(0xFFFFFFFFu, ers, my);
+                const uint32_t off = __shfl_sync(0xFFFFFFFFu, eoff, my);
+                owner += my;
+                const uint32_t t1 = __ldg(&g.rset_tile[r + 1]);
+                const uint32_t tile = __ldg(&g.rset_tile[r]) + (s - off) * 32 + lane;
+                const uint32_t fb = (__ldcg(&fprev[r >> 2]) >> (8 * (r & 3))) & 0xFFu;
+                // the rset's column labels, lane k < 8 holds column r*8+k
+                const uint32_t cv = r * 8 + (lane & 7);
+                const uint32_t cl = (lane < 8 && cv < g.n) ? __ldcg(&a.labels[cv]) : 0xFFFFFFFFu;
+                uint32_t col[8];
 #pragma unroll
-                for (uint32_t st = 16; st > 0; st >>= 1) {
-                    const uint32_t cand = lo + st;
-                    const uint32_t b = __shfl_sync(0xFFFFFFFFu, eoff, cand & 31);
-                    if (cand < 32 && b <= pos) lo = cand;
-                }
-                const uint32_t r = __shfl_sync(0xFFFFFFFFu, ers, lo);
-                const uint32_t off = __shfl_sync(0xFFFFFFFFu, eoff, lo);
-                owner += __shfl_sync(0xFFFFFFFFu, lo, 31);
-                const uint32_t tile = __ldg(&g.rset_tile[r]) + (pos - off);
-                const bool bad = pos < Uin && (pos < off || tile >= __ldg(&g.rset_tile[r + 1]));
-                if (bad) set_error(c, BLEST_ERR_DEVICE_INDEX);
-                if (pos < Uin && !bad) {
-                    const uint32_t fb = (__ldcg(&fprev[r >> 2]) >> (8 * (r & 3))) & 0xFFu;
+                for (int j = 0; j < 8; ++j) col[j] = __shfl_sync(0xFFFFFFFFu, cl, j);
+                if (tile < t1 && fb) {
                     const uint4 rows = ld_stream(&g.row4[tile]);
                     const uint32_t mask = ld_stream(&g.masks[tile]);
                     const uint32_t rowk[4] = {rows.x, rows.y, rows.z, rows.w};
 #pragma unroll
                     for (uint32_t kk = 0; kk < 4; ++kk) {
-                        uint32_t hb = (mask >> (8 * kk)) & fb & 0xFFu;
+                        const uint32_t hb = (mask >> (8 * kk)) & fb & 0xFFu;
                         if (!hb) continue;
                         const uint32_t row = rowk[kk];
                         if (row >= g.n) {
                             set_error(c, BLEST_ERR_DEVICE_INDEX);
                             continue;
                         }
-                        uint32_t m = __ldcg(&a.labels[row]);
-                        const uint32_t cur = m;
-                        while (hb) {
-                            const uint32_t col = r * 8 + (__ffs(hb) - 1);
-                            m = min(m, __ldcg(&a.labels[col]));
-                            hb &= hb - 1;
-                        }
-                        if (m < cur) {
+                        uint32_t m = 0xFFFFFFFFu;
+#pragma unroll
+                        for (int j = 0; j < 8; ++j)
+                            if ((hb >> j) & 1u) m = min(m, col[j]);
+                        if (m < __ldcg(&a.labels[row])) {
                             const uint32_t old = atomicMin(&a.labels[row], m);
                             if (m < old) {
                                 ++changes;

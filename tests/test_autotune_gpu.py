@@ -25,4 +25,4 @@ def test_tune_bfs_and_mbfs(tmp_path, gpu):
     p2, table2 = tune_bfs(g, src, space=space, cache=cache)  # from the cache
     assert table2 == table and p2.blocks_per_sm == p.blocks_per_sm
     best, mtable = tune_mbfs(g, src, cache=cache)
-    assert best["group_width"] in (32, 64, 128) and len(mtable) == 6
+    assert best["group_width"] in (32, 64, 128) and len(mtable) == 18
