@@ -180,6 +180,116 @@ std::vector<uint32_t> order_jaccard_window(const Csc& g, uint32_t slice_size, ui
     return inv;
 }
 
+namespace {
+
+// Breadth-first search that appends vertices to q in exactly the order of
+// the reference's sequential FIFO loop (CSC.cuh:994-1057 and :1082-1139):
+// a vertex's discoverer is the first vertex in queue order that has it as
+// a neighbour, at its first adjacency position; a parent's children are
+// appended in adjacency order (then, if `sort_children`, reordered by the
+// same std::sort on ascending degree as the reference). Levels with many
+// vertices are processed in parallel: every parent claims its unmarked
+// neighbours with an atomic minimum of (queue position, adjacency index),
+// the claims are counted per parent, prefix-summed into positions and
+// written; small levels run the sequential loop itself.
+class OrderedBfs {
+public:
+    OrderedBfs(const uint32_t* ptrs, const uint32_t* inds, const uint32_t* degrees, uint32_t n)
+        : ptrs_(ptrs), inds_(inds), deg_(degrees), key_(n, ~0ull) {}
+
+    // BFS from q[qs] (already marked); `unmarked(v)` / `mark(v)` give the
+    // visited state. Fills q from qs on; returns the end and the start of
+    // the last non-empty level (and the number of levels).
+    template <class Unmarked, class Mark>
+    void run(std::vector<uint32_t>& q, uint32_t qs, bool sort_children, Unmarked unmarked, Mark mark,
+             uint32_t& qend, uint32_t& last_level, uint32_t& levels) {
+        uint32_t ls = qs, le = qs + 1;
+        levels = 1;
+        last_level = ls;
+        auto degAsc = [this](uint32_t a, uint32_t b) { return deg_[a] < deg_[b]; };
+        for (;;) {
+            uint64_t work = 0;
+            for (uint32_t i = ls; i < le && work < kParallelWork; ++i) work += ptrs_[q[i] + 1] - ptrs_[q[i]];
+            uint32_t ne = le;
+            if (work < kParallelWork) {
+                for (uint32_t i = ls; i < le; ++i) {
+                    const uint32_t u = q[i];
+                    const uint32_t first = ne;
+                    for (uint32_t p = ptrs_[u]; p < ptrs_[u + 1]; ++p) {
+                        const uint32_t v = inds_[p];
+                        if (unmarked(v)) {
+                            mark(v);
+                            q[ne++] = v;
+                        }
+                    }
+                    if (sort_children) std::sort(q.begin() + first, q.begin() + ne, degAsc);
+                }
+            } else {
+                const int64_t L = (int64_t)le - ls;
+                cnt_.assign((size_t)L + 1, 0);
+#pragma omp parallel for schedule(dynamic, 64)
+                for (int64_t x = 0; x < L; ++x) {
+                    const uint32_t u = q[ls + x];
+                    for (uint32_t p = ptrs_[u]; p < ptrs_[u + 1]; ++p) {
+                        const uint32_t v = inds_[p];
+                        if (!unmarked(v)) continue;
+                        const uint64_t k = ((uint64_t)(ls + x) << 32) | (p - ptrs_[u]);
+                        uint64_t cur = __atomic_load_n(&key_[v], __ATOMIC_RELAXED);
+                        while (k < cur &&
+                               !__atomic_compare_exchange_n(&key_[v], &cur, k, true, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
+                        }
+                    }
+                }
+#pragma omp parallel for schedule(dynamic, 64)
+                for (int64_t x = 0; x < L; ++x) {
+                    const uint32_t u = q[ls + x];
+                    uint32_t c = 0;
+                    for (uint32_t p = ptrs_[u]; p < ptrs_[u + 1]; ++p) {
+                        const uint32_t v = inds_[p];
+                        if (unmarked(v) && key_[v] == (((uint64_t)(ls + x) << 32) | (p - ptrs_[u]))) ++c;
+                    }
+                    cnt_[x + 1] = c;
+                }
+                for (int64_t x = 0; x < L; ++x) cnt_[x + 1] += cnt_[x];
+                ne = le + (uint32_t)cnt_[L];
+#pragma omp parallel for schedule(dynamic, 64)
+                for (int64_t x = 0; x < L; ++x) {
+                    const uint32_t u = q[ls + x];
+                    uint32_t w = le + (uint32_t)cnt_[x];
+                    const uint32_t first = w;
+                    for (uint32_t p = ptrs_[u]; p < ptrs_[u + 1]; ++p) {
+                        const uint32_t v = inds_[p];
+                        if (unmarked(v) && key_[v] == (((uint64_t)(ls + x) << 32) | (p - ptrs_[u]))) q[w++] = v;
+                    }
+                    if (sort_children) std::sort(q.begin() + first, q.begin() + w, degAsc);
+                }
+#pragma omp parallel for schedule(static, 4096)
+                for (int64_t i = le; i < (int64_t)ne; ++i) {
+                    const uint32_t v = q[i];
+                    key_[v] = ~0ull;
+                    mark(v);
+                }
+            }
+            if (ne == le) break;
+            ls = le;
+            le = ne;
+            last_level = ls;
+            ++levels;
+        }
+        qend = le;
+    }
+
+private:
+    static constexpr uint64_t kParallelWork = 1u << 16;  // edges of a level worth a parallel pass
+    const uint32_t* ptrs_;
+    const uint32_t* inds_;
+    const uint32_t* deg_;
+    std::vector<uint64_t> key_;
+    std::vector<uint64_t> cnt_;
+};
+
+}  // namespace
+
 // Ordering of CSC::rcm (CSC.cuh:1059-1142) with the pseudo-peripheral
 // start of CSC.cuh:994-1057. As in the reference the BFS order is used
 // without reversal (inversePermutation[u] = position in the Cuthill-McKee
@@ -188,7 +298,9 @@ std::vector<uint32_t> order_jaccard_window(const Csc& g, uint32_t slice_size, ui
 // restart vertex is drawn from the last BFS level with the C library
 // rand() sequence, reproduced by GlibcRand from `rand_seed` (1 = the
 // reference's never-seeded state). The per-call O(n) marker allocation of
-// the reference is replaced by one stamped marker array.
+// the reference is replaced by one stamped marker array, and every BFS
+// runs level by level with large levels in parallel (OrderedBfs), giving
+// the same queue order as the sequential loop.
 std::vector<uint32_t> order_rcm(const Csc& g0, uint32_t rand_seed) {
     const Csc* gp = &g0;
     Csc sym;
@@ -200,63 +312,40 @@ std::vector<uint32_t> order_rcm(const Csc& g0, uint32_t rand_seed) {
     const uint32_t n = g.n;
     const uint32_t* ptrs = g.col_ptrs.data();
     const uint32_t* inds = g.rows.data();
-    std::vector<uint32_t> inv(n, 0), degrees(n), visited(n, 0), q(n), nbrs(n), stamp(n, 0);
+    std::vector<uint32_t> inv(n, 0), degrees(n), visited(n, 0), q(n), stamp(n, 0);
     for (uint32_t i = 0; i < n; ++i) degrees[i] = ptrs[i + 1] - ptrs[i];
     GlibcRand rng(rand_seed);
     uint32_t marker = 1;
+    OrderedBfs bfs(ptrs, inds, degrees.data(), n);
 
     auto pseudoPeripheral = [&](uint32_t startNode) -> uint32_t {
         uint32_t maxLevel = 0, trial = 0;
         while (trial < 10) {
             ++marker;
+            const uint32_t mk = marker;
             q[0] = startNode;
-            stamp[startNode] = marker;
-            uint32_t qe = 1, qs = 0, levelStart = 0, levelEnd = qe, levelid = 1;
-            while (qs < qe) {
-                const uint32_t u = q[qs++];
-                for (uint32_t p = ptrs[u]; p < ptrs[u + 1]; ++p) {
-                    const uint32_t v = inds[p];
-                    if (stamp[v] != marker) {
-                        stamp[v] = marker;
-                        q[qe++] = v;
-                    }
-                }
-                if (qs == levelEnd && qs < qe) {
-                    levelStart = qs;
-                    levelEnd = qe;
-                    levelid++;
-                }
-            }
+            stamp[startNode] = mk;
+            uint32_t qe = 0, last = 0, levelid = 0;
+            bfs.run(q, 0, false, [&](uint32_t v) { return stamp[v] != mk; }, [&](uint32_t v) { stamp[v] = mk; }, qe,
+                    last, levelid);
             if (levelid == maxLevel) trial++;
             else trial = 0;
             maxLevel = levelid;
-            startNode = q[levelStart + ((uint32_t)rng() % (levelEnd - levelStart))];
+            startNode = q[last + ((uint32_t)rng() % (qe - last))];
         }
         return startNode;
     };
 
-    auto compAsc = [&](uint32_t a, uint32_t b) { return degrees[a] < degrees[b]; };
     uint32_t permuted = 0;
     for (uint32_t i = 0; i < n; ++i) {
         if (visited[i] == 1) continue;
         const uint32_t start = pseudoPeripheral(i);
-        uint32_t qs = 0, qe = 0;
-        q[qe++] = start;
+        q[0] = start;
         visited[start] = 1;
-        while (qs < qe) {
-            const uint32_t u = q[qs++];
-            inv[u] = permuted++;
-            uint32_t k = 0;
-            for (uint32_t p = ptrs[u]; p < ptrs[u + 1]; ++p) {
-                const uint32_t v = inds[p];
-                if (visited[v] == 0) {
-                    nbrs[k++] = v;
-                    visited[v] = 1;
-                }
-            }
-            std::sort(nbrs.begin(), nbrs.begin() + k, compAsc);
-            for (uint32_t x = 0; x < k; ++x) q[qe++] = nbrs[x];
-        }
+        uint32_t qe = 0, last = 0, levels = 0;
+        bfs.run(q, 0, true, [&](uint32_t v) { return visited[v] == 0; }, [&](uint32_t v) { visited[v] = 1; }, qe, last,
+                levels);
+        for (uint32_t x = 0; x < qe; ++x) inv[q[x]] = permuted++;
     }
     return inv;
 }

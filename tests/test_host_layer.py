@@ -4,6 +4,7 @@ reference's own outputs stored in tests/golden/host_*.npz
 import numpy as np
 import pytest
 
+import oracle as O
 from blest_b200 import BlestError, Bvss, Csc, load_ordering, save_ordering
 
 
@@ -161,3 +162,15 @@ def test_relabel_dense():
     d, k = relabel_dense(lab)
     assert k == 3
     np.testing.assert_array_equal(d, [0, 0, 1, 1, 0, 2, 2])
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference harness not built")
+@pytest.mark.parametrize("make", [lambda: Csc.rmat(16, 16, seed=2, permute_seed=2),
+                                  lambda: Csc.er(1 << 16, 16 << 15, seed=3),
+                                  lambda: Csc.grid(300, 200, 0.3, 0.001, seed=3)])
+def test_rcm_matches_reference_on_parallel_levels(make):
+    """RCM orders big enough that levels run on the parallel path (more
+    than 2^16 edges per level) equal the reference's sequential order."""
+    c = make()
+    want = O.RefGraph.from_csc(c.n, c.col_ptrs, c.rows).reorder("rcm")
+    np.testing.assert_array_equal(c.reorder("rcm"), want)
