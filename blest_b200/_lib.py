@@ -1,6 +1,6 @@
 """ctypes bindings of libblest_b200.so (the C ABI declared in include/blest.h).
 
-The shared library is built in-tree (python -m blest_b200.build). There is
+The shared library is built in-tree (python blest_b200/build.py). There is
 no Python or CPU fallback for the device entry points: if the library is
 missing, importing this module raises.
 """
@@ -14,7 +14,7 @@ LIB_PATH = _PKG / "libblest_b200.so"
 
 if not LIB_PATH.exists():
     raise ImportError(
-        f"{LIB_PATH} is missing: build it with `python -m blest_b200.build` "
+        f"{LIB_PATH} is missing: build it with `python blest_b200/build.py` "
         "(the BFS/CC/MBFS path has no CPU fallback)")
 
 lib = C.CDLL(str(LIB_PATH))

@@ -1,6 +1,7 @@
 """Build libblest_b200.so in-tree: host C++ (g++/OpenMP) + sm_100a CUDA
 (nvcc -gencode arch=compute_100a,code=sm_100a), linked into one shared
-library next to this file. Usage: python -m blest_b200.build [--force]."""
+library next to this file. Usage: python blest_b200/build.py [--force | --ptxas]
+(by path: importing the package needs the library this builds)."""
 from __future__ import annotations
 
 import concurrent.futures as cf

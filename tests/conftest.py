@@ -14,8 +14,12 @@ def pytest_configure(config):
 
 
 def _ensure_built():
-    from blest_b200 import build as B
-    B.build()
+    # build.py by path: the package import needs the library built here
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("blest_b200_build", ROOT / "blest_b200" / "build.py")
+    builder = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(builder)
+    builder.build()
     import oracle
     if not oracle.ORACLE_SO.exists():
         oracle.build(ref=False)
