@@ -45,6 +45,9 @@ WORKLOADS = {
                  "2D 4096x4096 grid, 5% edges deleted, 0.1% shortcuts, RCM, 32 seeded sources"),
     "er25": ("bfs", ("er", 25, 32), "rcm", 0, 32, "Erdos-Renyi 2^25 vertices avg degree 32, RCM, 32 sources"),
     "cc_rmat24": ("cc", ("rmat", 24, 16), "jaccard", 65536, 0, "connected components, RMAT scale 24"),
+    "cc_grid4096": ("cc", ("grid", 4096, 4096), "rcm", 0, 0,
+                    "connected components, 2D 4096x4096 grid, 5% edges deleted, 0.1% shortcuts, RCM"),
+    "cc_er25": ("cc", ("er", 25, 32), "rcm", 0, 0, "connected components, Erdos-Renyi 2^25 avg degree 32, RCM"),
     "serving": ("serving", None, None, 0, 0,
                 "query server: resident graphs RMAT 18/20/22, grid 1024^2, ER 2^22 deg 16; Poisson arrivals, "
                 "80% BFS (uniform seeded source) / 20% CC, graph uniform; rate sweep"),
@@ -68,11 +71,14 @@ def log(*a):
 # ----------------------------------------------------------------- graph prep
 def prepare(workload: str, cache_dir: Path, rank: int, world: int):
     """Build (or load from the per-run cache) the reordered CSC, BVSS and
-    pull CSR. Rank 0 builds; other ranks wait for the cache files."""
+    pull CSR. Rank 0 builds; other ranks wait for the cache files. Workloads
+    on the same graph share one cache entry; the sources of every such
+    workload's count are sampled when the graph is built."""
     from blest_b200 import Bvss, Csc
     kind, gen, order, window, nsrc, _ = WORKLOADS[workload]
     cache_dir.mkdir(parents=True, exist_ok=True)
-    tag = cache_dir / workload
+    tag = cache_dir / f"{'_'.join(map(str, gen))}_{order}_{window}"
+    counts = sorted({w[4] for w in WORKLOADS.values() if w[1:4] == (gen, order, window) and w[4]})
     done = Path(str(tag) + ".ready")
     if rank == 0 and not done.exists():
         t0 = time.time()
@@ -84,7 +90,7 @@ def prepare(workload: str, cache_dir: Path, rank: int, world: int):
             n = 1 << gen[1]
             csc = Csc.er(n, n * gen[2] // 2, seed=SEED)
         t1 = time.time()
-        sources = csc.sample_sources(nsrc, SEED) if nsrc else np.zeros(0, np.uint32)
+        samples = {k: csc.sample_sources(k, SEED) for k in counts}
         inv = csc.reorder(order, window=window or 65536)
         t2 = time.time()
         bvss = Bvss.build(csc)
@@ -93,7 +99,8 @@ def prepare(workload: str, cache_dir: Path, rank: int, world: int):
             f"n={csc.n} nnz={csc.nnz} social={csc.is_social}")
         csc.save_bin(str(tag) + "_csc.bin")
         bvss.save_bin(str(tag) + "_bvss.bin")
-        np.save(str(tag) + "_sources.npy", inv[sources] if nsrc else sources)
+        for k, src in samples.items():
+            np.save(str(tag) + f"_sources{k}.npy", inv[src])
         done.write_text("ok")
     else:
         deadline = time.time() + 3600
@@ -103,7 +110,7 @@ def prepare(workload: str, cache_dir: Path, rank: int, world: int):
             time.sleep(1.0)
         csc = Csc.load_bin(str(tag) + "_csc.bin")
         bvss = Bvss.load_bin(str(tag) + "_bvss.bin")
-    sources = np.load(str(tag) + "_sources.npy")
+    sources = np.load(str(tag) + f"_sources{nsrc}.npy") if nsrc else np.zeros(0, np.uint32)
     csr = csc if csc.is_symmetric() else csc.transpose()
     return csc, bvss, csr, sources
 
