@@ -144,12 +144,20 @@ class ClockSampler:
         self.lines: list[str] = []
 
     def __enter__(self):
+        """Start sampling every 20 ms and wait (up to 3 s) for the first
+        reading, so that even a short timed region gets samples; readings
+        taken before the region starts are left out of the summary."""
+        self.first = 0
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "20"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            deadline = time.time() + 3.0
+            while not self.lines and time.time() < deadline and self.proc.poll() is None:
+                time.sleep(0.005)
+            self.first = len(self.lines)
         except FileNotFoundError:
             self.proc = None
         return self
@@ -169,7 +177,8 @@ class ClockSampler:
     def summary(self) -> dict:
         sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        lines = self.lines[self.first:] or self.lines[-1:]
+        for line in lines:
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue

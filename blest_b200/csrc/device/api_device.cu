@@ -390,8 +390,11 @@ int blest_bfs_ws(blest_workspace* ws, uint32_t source, uint32_t* levels_out, uin
         BLEST_CUDA(cudaEventRecord(w.ev_start, s));
         blest::launch_bfs(g, w, source, dl, dp, p, s);
         BLEST_CUDA(cudaEventRecord(w.ev_stop, s));
-        BLEST_CUDA(cudaMemcpyAsync(w.host_counters, w.counters, sizeof(blest::dev::RunCounters),
-                                   cudaMemcpyDeviceToHost, s));
+        // the run's status is copied back here only for a blocking call; an
+        // asynchronous one reads it in blest_workspace_sync
+        if (!async)
+            BLEST_CUDA(cudaMemcpyAsync(w.host_counters, w.counters, sizeof(blest::dev::RunCounters),
+                                       cudaMemcpyDeviceToHost, s));
         if (out_mem == BLEST_MEM_HOST) {
             BLEST_CUDA(cudaMemcpyAsync(levels_out, dl, 4ull * g->d.n, cudaMemcpyDeviceToHost, s));
             if (parents_out) BLEST_CUDA(cudaMemcpyAsync(parents_out, dp, 4ull * g->d.n, cudaMemcpyDeviceToHost, s));
@@ -414,6 +417,8 @@ int blest_workspace_sync(blest_workspace* ws, blest_bfs_stats* stats) {
         if (!ws->pending) return;
         BLEST_CUDA(cudaStreamSynchronize(ws->stream));
         ws->pending = false;
+        BLEST_CUDA(cudaMemcpy(ws->w.host_counters, ws->w.counters, sizeof(blest::dev::RunCounters),
+                              cudaMemcpyDeviceToHost));
         float ms = 0;
         BLEST_CUDA(cudaEventElapsedTime(&ms, ws->w.ev_start, ws->w.ev_stop));
         fill_bfs_stats(ws->w, ws->pending_src, ms, stats);

@@ -21,7 +21,9 @@
 
 #include <algorithm>
 #include <chrono>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <string>
 
 #include "common.cuh"
@@ -74,8 +76,11 @@ __device__ __forceinline__ void summary_set(const BfsArgs& a, uint32_t* sum, uin
     atomicOr(&sum[sb >> 5], 1u << (sb & 31));
 }
 
-// Neighbours a lane scans alone in the pull phase before the warp takes over.
+// Neighbours a lane scans alone in the pull phase before the warp takes over,
+// and how many of them it has in flight at once (a warp waits for its
+// slowest lane, so fewer, wider rounds finish sooner).
 constexpr uint32_t kPullLaneScan = 32;
+constexpr uint32_t kPullUnroll = 4;
 // Neighbours per piece of a heavy (very long) in-neighbour list.
 constexpr uint32_t kHeavyChunk = 256;
 
@@ -167,26 +172,33 @@ __device__ __forceinline__ void flush_enqueue(const BfsArgs& a, Enqueue& q, int 
 // Claim vertex `row` for `level`; the atomicOr on visited decides the
 // single winner, which records level/parent, sets the frontier bit and,
 // when it is the first new vertex of its rset this level, queues the rset.
+// `precheck`: read the visited word first and skip the atomic for visited
+// rows (saves contended atomics in big levels; small levels skip the read,
+// one round trip less on their critical path).
 template <bool ALIGNED, bool PARENTS>
 __device__ __forceinline__ void discover(const BfsArgs& a, uint32_t* fcur, uint32_t* fsum, uint32_t row,
                                          uint32_t parent, uint32_t level, Enqueue& q, uint32_t& disc,
-                                         uint64_t& deg) {
+                                         uint64_t& deg, bool precheck) {
     if (row >= a.g.n) {
         set_error(a.ctr, BLEST_ERR_DEVICE_INDEX);
         return;
     }
     const uint32_t w = row >> 5, b = 1u << (row & 31);
-    if (__ldcg(&a.visited[w]) & b) return;
+    if (precheck && (__ldcg(&a.visited[w]) & b)) return;
     const uint32_t old = atomicOr(&a.visited[w], b);
     if (old & b) return;
     a.levels[row] = level;
     if (PARENTS) a.parents[row] = parent;
     ++disc;
-    deg += __ldg(&a.g.csr_ptrs[row + 1]) - __ldg(&a.g.csr_ptrs[row]);
+    // degree and rset tile bounds are loaded together with the frontier
+    // atomic (one round trip instead of three)
+    const uint32_t r = row >> 3;
+    const uint32_t d0 = __ldg(&a.g.csr_ptrs[row]), d1 = __ldg(&a.g.csr_ptrs[row + 1]);
+    const uint32_t t0 = __ldg(&a.g.rset_tile[r]), t1 = __ldg(&a.g.rset_tile[r + 1]);
     const uint32_t oldF = atomicOr(&fcur[w], b);
+    deg += d1 - d0;
     if (((oldF >> (row & 24)) & 0xFFu) == 0) {
-        const uint32_t r = row >> 3;
-        const uint32_t units = rset_units<ALIGNED>(a.g, r);
+        const uint32_t units = ALIGNED ? (t1 - t0 + 31) / 32 : t1 - t0;
         if (units) {
             q.rset[q.cnt++] = r;
             q.units += units;
@@ -455,6 +467,7 @@ __global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(BfsArgs a) {
 
         if (dir == BLEST_DIR_PUSH) {
             const uint32_t total = U1 - U2;
+            const bool precheck = total > (ALIGNED ? 64u : 2048u);  // level larger than ~2k tiles
             const uint32_t per = ALIGNED ? 1u : 32u;  // units per warp step
             const uint32_t steps = (total + per - 1) / per;
             const uint32_t k = (steps + nwarps - 1) / nwarps;
@@ -481,7 +494,7 @@ __global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(BfsArgs a) {
                             if (hits & (1u << kk)) {
                                 const uint32_t hb = (cur.mask >> (8 * kk)) & cur.fb & 0xFFu;
                                 discover<ALIGNED, PARENTS>(a, fcur, fsum, rowk[kk], cur.r * 8 + (__ffs(hb) - 1),
-                                                           level, q, disc, deg);
+                                                           level, q, disc, deg, precheck);
                             }
                         }
                     }
@@ -530,15 +543,16 @@ __global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(BfsArgs a) {
                     pe = re;
                     p = pb;
                     const uint32_t cap = pb + min(pe - pb, kPullLaneScan);
-                    for (; p < cap && !found; p += 4) {
-                        uint32_t v[4];
-                        bool f[4];
+                    for (; p < cap && !found; p += kPullUnroll) {
+                        uint32_t v[kPullUnroll];
+                        bool f[kPullUnroll];
 #pragma unroll
-                        for (uint32_t j = 0; j < 4; ++j) v[j] = p + j < pe ? __ldg(&g.csr_ids[p + j]) : kUnreached;
+                        for (uint32_t j = 0; j < kPullUnroll; ++j)
+                            v[j] = p + j < pe ? __ldg(&g.csr_ids[p + j]) : kUnreached;
 #pragma unroll
-                        for (uint32_t j = 0; j < 4; ++j) f[j] = v[j] != kUnreached && in_frontier(v[j]);
+                        for (uint32_t j = 0; j < kPullUnroll; ++j) f[j] = v[j] != kUnreached && in_frontier(v[j]);
 #pragma unroll
-                        for (uint32_t j = 0; j < 4; ++j) {
+                        for (uint32_t j = 0; j < kPullUnroll; ++j) {
                             if (!found && f[j]) {
                                 found = true;
                                 parent = v[j];
@@ -702,12 +716,25 @@ void launch_variant(const blest_graph* g, const dev::BfsArgs& args, int blocks_p
                     uint32_t grid_cap, cudaStream_t s) {
     auto kern = dev::bfs_persistent_kernel<ALIGNED, MMA, PARENTS>;
     const size_t smem = 4ull * args.sum_words;
-    // Always the same (maximum) value: calls for graphs of different sizes
-    // may run concurrently from several threads.
-    BLEST_CUDA(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)kSummaryMaxBytes));
+    // Per (device, block size, shared memory): the attribute is set once
+    // (always the maximum, so concurrent calls for graphs of different sizes
+    // agree) and the occupancy is asked once; both are fixed per device.
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, size_t>, int> occupancy;
     int maxBlocks = 0;
-    BLEST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxBlocks, kern, threads, smem));
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        const auto key = std::make_tuple(g->device, threads, smem);
+        const auto it = occupancy.find(key);
+        if (it != occupancy.end()) {
+            maxBlocks = it->second;
+        } else {
+            BLEST_CUDA(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)kSummaryMaxBytes));
+            BLEST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxBlocks, kern, threads, smem));
+            occupancy[key] = maxBlocks;
+        }
+    }
     if (maxBlocks < 1) throw Error(BLEST_ERR_CUDA, "BFS kernel cannot be resident with this block size");
     const int bps = blocks_per_sm > 0 ? std::min(blocks_per_sm, maxBlocks) : maxBlocks;
     const int grid = cooperative_grid(bps, g->sm_count, grid_cap);

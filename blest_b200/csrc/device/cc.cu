@@ -132,7 +132,9 @@ __device__ __forceinline__ uint32_t cc_find_owner(const uint32_t* q_off, uint32_
     return lo + __popc(__ballot_sync(0xFFFFFFFFu, ok)) - 1;
 }
 
-__global__ void __launch_bounds__(512) cc_persistent_kernel(CcArgs a) {
+// Three blocks of 512 threads per SM: the register bound (42) keeps the
+// pointer jump from costing a third of the resident threads.
+__global__ void __launch_bounds__(512, 3) cc_persistent_kernel(CcArgs a) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t nth = gridDim.x * blockDim.x;
@@ -206,6 +208,13 @@ __global__ void __launch_bounds__(512) cc_persistent_kernel(CcArgs a) {
                         for (int j = 0; j < 8; ++j)
                             if ((hb >> j) & 1u) m = min(m, col[j]);
                         if (m < __ldcg(&a.labels[row])) {
+                            // one pointer jump: m is the id of a vertex of the
+                            // same component, so its label is a valid, possibly
+                            // smaller, label too (the fixpoint, the component's
+                            // minimum id, is unchanged; long chains such as a
+                            // grid numbered outward from a corner shrink by
+                            // doubling instead of one hop per iteration).
+                            m = min(m, __ldcg(&a.labels[m]));
                             const uint32_t old = atomicMin(&a.labels[row], m);
                             if (m < old) {
                                 ++changes;

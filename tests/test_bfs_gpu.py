@@ -85,3 +85,28 @@ def test_device_output_buffer(gpu):
     np.testing.assert_array_equal(lv, O.bfs_csc(csc.n, csc.col_ptrs, csc.rows, 7))
     assert O.check_parents(csc.n, csc.col_ptrs, csc.rows, 7, lv, par.cpu().numpy().view(np.uint32)) == 0
     assert st.no_visited == int((lv != O.UNREACHED).sum())
+
+
+def test_async_runs_then_sync_reports_the_last(gpu):
+    """Asynchronous BFS calls queue no status copy; blest_workspace_sync
+    waits and reports the last run's statistics."""
+    import torch
+
+    from blest_b200 import Csc, Workspace
+    from graphs import prepared
+    csc, bvss, csr = prepared(Csc.rmat(12, 16, seed=9, permute_seed=4), "jaccard", 1024)
+    g = Graph(bvss, csr)
+    ws = Workspace(g)
+    out = torch.empty(csc.n, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.Stream()
+    sources = csc.sample_sources(6, seed=3)
+    for s in sources:
+        ws.bfs_async(int(s), out.data_ptr(), stream.cuda_stream)
+    st = ws.sync()
+    want = O.bfs_csc(csc.n, csc.col_ptrs, csc.rows, int(sources[-1]))
+    np.testing.assert_array_equal(out.cpu().numpy().view(np.uint32), want)
+    reached = want != O.UNREACHED
+    assert st.source_vertex == int(sources[-1])
+    assert st.no_visited == int(reached.sum())
+    assert st.total_levels == int(want[reached].max()) + 1
+    ws.close()
