@@ -424,10 +424,17 @@ __global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(BfsArgs a) {
             // vertices. As in Beamer's heuristic, only a growing frontier
             // starts a pull phase: late levels have tiny m_u, and a pull
             // level there would scan every vertex word for a few vertices.
+            // Back to push also needs the push work (the frontier's tiles,
+            // known now) to be below the pull's fixed cost (one visit per
+            // 32-vertex word): a uniform-degree graph's last levels have a
+            // frontier under n / beta whose tiles still outnumber the words
+            // many times, while almost nothing is left unvisited.
             const double mf = (double)(G1 - G2), mu = (double)(g.degree_total - G1);
             const bool growing = nf > nf_prev;
             if (dir == BLEST_DIR_PUSH && mf * a.alpha > mu && growing) dir = BLEST_DIR_PULL;
-            else if (dir == BLEST_DIR_PULL && (double)nf * a.beta < (double)g.n) dir = BLEST_DIR_PUSH;
+            else if (dir == BLEST_DIR_PULL && (double)nf * a.beta < (double)g.n &&
+                     (U1 - U2) * (ALIGNED ? 32ull : 1ull) < (uint64_t)((g.n + 31) / 32))
+                dir = BLEST_DIR_PUSH;
         }
         nf_prev = nf;
         if (a.trace && tid == 0 && level <= BLEST_TRACE_CAPACITY) {
