@@ -51,6 +51,10 @@ WORKLOADS = {
     "serving": ("serving", None, None, 0, 0,
                 "query server: resident graphs RMAT 18/20/22, grid 1024^2, ER 2^22 deg 16; Poisson arrivals, "
                 "80% BFS (uniform seeded source) / 20% CC, graph uniform; rate sweep"),
+    "mbfs_rmat20": ("mbfs", ("rmat", 20, 16), "jaccard", 65536, 128,
+                    "multi-source BFS, RMAT scale 20 ef 16, Jaccard window 65536, 128 seeded sources (one group; "
+                    "the profiling case)"),
+    "cc_rmat20": ("cc", ("rmat", 20, 16), "jaccard", 65536, 0, "connected components, RMAT scale 20 (profiling case)"),
     "mbfs_rmat22": ("mbfs", ("rmat", 22, 16), "jaccard", 65536, 1024,
                     "multi-source BFS, RMAT scale 22 ef 16, Jaccard window 65536, 1024 seeded sources "
                     "in bit-packed groups of 128"),
@@ -651,7 +655,8 @@ def run_serving(args, rank, world):
     pools = []
     for _, csc, _, _, _ in graphs:
         q = qmod.Queue()
-        for _ in range(args.buffers):
+        # at most ~2 GB of pinned result buffers per graph
+        for _ in range(max(8, min(args.buffers, int(2e9 // (4 * csc.n))))):
             q.put(torch.empty(csc.n, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32))
         pools.append(q)
     rates = [float(r) for r in args.rates.split(",")]
