@@ -605,6 +605,11 @@ SERVING_GRAPHS_FULL = SERVING_GRAPHS[:3] + [("rmat24", ("rmat", 24, 16), "jaccar
                                             ("er24", ("er", 24, 32), "rcm")]
 
 
+SERVING_FULL_DESCRIPTION = ("query server: 8 resident graphs, RMAT scales 18/20/22/24, grids 1024^2 and 4096^2, "
+                            "ER 2^22 deg 16 and 2^24 deg 32; Poisson arrivals, 80% BFS (uniform seeded source) / "
+                            "20% CC, graph uniform; every result copied to pinned host memory; rate sweep")
+
+
 def build_graph(gen, order):
     from blest_b200 import Bvss, Csc
     if gen[0] == "rmat":
@@ -729,7 +734,8 @@ def run_serving(args, rank, world):
         "value": head["p50_ms"], "unit": "ms", "n_gpus": 1, "steps": len(sweep), "warmup": 0,
         "ms_per_step": None, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic (seeded generators; Poisson arrivals from a fixed seed)",
-        "config": {"workload": "serving", "description": WORKLOADS["serving"][5],
+        "config": {"workload": "serving",
+                   "description": (SERVING_FULL_DESCRIPTION if args.serving_full else WORKLOADS["serving"][5]),
                    "graphs": [x[0] for x in graphs], "lanes": args.lanes, "max_batch": 128, "sweep": sweep},
         "e2e": {"value": head["p50_ms"], "unit": "ms", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
                 "note": "latency measured from submit to result in host memory"},
