@@ -472,6 +472,13 @@ __global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(BfsArgs a) {
         uint32_t disc = 0;
         uint64_t deg = 0;
 
+        // Lazy push (levels-only runs): when the frontier's edges exceed n/4
+        // the level discovers a large part of the graph; then a hit only ORs
+        // the row into fcur (one atomic whose result nobody waits for) and a
+        // word sweep after a barrier keeps the unvisited bits, marks them
+        // visited, writes their levels and queues their rsets -- instead of
+        // the claim/record/enqueue chain per discovered vertex.
+        const bool lazy = !PARENTS && dir == BLEST_DIR_PUSH && (G1 - G2) > (uint64_t)(g.n / 4);
         if (dir == BLEST_DIR_PUSH) {
             const uint32_t total = U1 - U2;
             const bool precheck = total > (ALIGNED ? 64u : 2048u);  // level larger than ~2k tiles
@@ -500,12 +507,69 @@ __global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(BfsArgs a) {
                         for (uint32_t kk = 0; kk < 4; ++kk) {
                             if (hits & (1u << kk)) {
                                 const uint32_t hb = (cur.mask >> (8 * kk)) & cur.fb & 0xFFu;
-                                discover<ALIGNED, PARENTS>(a, fcur, fsum, rowk[kk], cur.r * 8 + (__ffs(hb) - 1),
-                                                           level, q, disc, deg, precheck);
+                                const uint32_t row = rowk[kk];
+                                if (lazy) {
+                                    if (row >= g.n) {
+                                        set_error(c, BLEST_ERR_DEVICE_INDEX);
+                                    } else if (!((__ldcg(&a.visited[row >> 5]) >> (row & 31)) & 1u)) {
+                                        atomicOr(&fcur[row >> 5], 1u << (row & 31));
+                                    }
+                                } else {
+                                    discover<ALIGNED, PARENTS>(a, fcur, fsum, row, cur.r * 8 + (__ffs(hb) - 1), level, q,
+                                                               disc, deg, precheck);
+                                }
                             }
                         }
                     }
                     flush_enqueue<ALIGNED>(a, q, kEnqueueCap - 4);
+                }
+            }
+            if (lazy) {
+                if (!grid_barrier(c)) return;
+                // Sweep: lane j of a warp takes word base + j (candidates,
+                // visited, rsets to queue); then the warp walks those 32
+                // words with one lane per vertex for coalesced level writes
+                // and degree reads.
+                const uint32_t W = (g.n + 31) / 32;
+                for (uint32_t base = warp * 32; base < W; base += nwarps * 32) {
+                    const uint32_t wi = base + lane;
+                    uint32_t nw = 0;
+                    bool queued = false;
+                    if (wi < W) {
+                        const uint32_t cand = __ldcg(&fcur[wi]);
+                        if (cand) {
+                            const uint32_t vis = __ldcg(&a.visited[wi]);
+                            nw = cand & ~vis;
+                            fcur[wi] = nw;
+                            if (nw) a.visited[wi] = vis | nw;
+                        }
+                    }
+#pragma unroll
+                    for (uint32_t kk = 0; kk < 4; ++kk) {
+                        if ((nw >> (8 * kk)) & 0xFFu) {
+                            const uint32_t r = wi * 4 + kk;
+                            const uint32_t units = rset_units<ALIGNED>(g, r);
+                            if (units) {
+                                q.rset[q.cnt++] = r;
+                                q.units += units;
+                                queued = true;
+                            }
+                        }
+                    }
+                    if (queued) summary_set(a, fsum, wi);
+                    flush_enqueue<ALIGNED>(a, q, kEnqueueCap - 4);
+                    uint32_t words = __ballot_sync(0xFFFFFFFFu, nw != 0);
+                    while (words) {
+                        const uint32_t j = __ffs(words) - 1;
+                        words &= words - 1;
+                        const uint32_t bits = __shfl_sync(0xFFFFFFFFu, nw, j);
+                        if ((bits >> lane) & 1u) {
+                            const uint32_t v = (base + j) * 32 + lane;
+                            a.levels[v] = level;
+                            ++disc;
+                            deg += __ldg(&g.csr_ptrs[v + 1]) - __ldg(&g.csr_ptrs[v]);
+                        }
+                    }
                 }
             }
         } else {
