@@ -424,16 +424,18 @@ __global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(BfsArgs a) {
             // vertices. As in Beamer's heuristic, only a growing frontier
             // starts a pull phase: late levels have tiny m_u, and a pull
             // level there would scan every vertex word for a few vertices.
-            // Back to push also needs the push work (the frontier's tiles,
-            // known now) to be below the pull's fixed cost (one visit per
+            // Back to push also needs the push work (the new frontier's
+            // edges m_f) to be under 8x the pull's fixed cost (one visit per
             // 32-vertex word): a uniform-degree graph's last levels have a
-            // frontier under n / beta whose tiles still outnumber the words
-            // many times, while almost nothing is left unvisited.
+            // frontier under n / beta whose edges outnumber the words 14-29x,
+            // while almost nothing is left unvisited; a grid after a pull
+            // level has at most ~5x and is better off pushing. (Edges, not
+            // tiles: full-padding tiles overstate a grid's push work.)
             const double mf = (double)(G1 - G2), mu = (double)(g.degree_total - G1);
             const bool growing = nf > nf_prev;
             if (dir == BLEST_DIR_PUSH && mf * a.alpha > mu && growing) dir = BLEST_DIR_PULL;
             else if (dir == BLEST_DIR_PULL && (double)nf * a.beta < (double)g.n &&
-                     (U1 - U2) * (ALIGNED ? 32ull : 1ull) < (uint64_t)((g.n + 31) / 32))
+                     mf < 8.0 * (double)((g.n + 31) / 32))
                 dir = BLEST_DIR_PUSH;
         }
         nf_prev = nf;
@@ -472,13 +474,13 @@ __global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(BfsArgs a) {
         uint32_t disc = 0;
         uint64_t deg = 0;
 
-        // Lazy push (levels-only runs): when the frontier's edges exceed n/4
+        // Lazy push (levels-only runs): when the frontier's edges exceed n/2
         // the level discovers a large part of the graph; then a hit only ORs
         // the row into fcur (one atomic whose result nobody waits for) and a
         // word sweep after a barrier keeps the unvisited bits, marks them
         // visited, writes their levels and queues their rsets -- instead of
         // the claim/record/enqueue chain per discovered vertex.
-        const bool lazy = !PARENTS && dir == BLEST_DIR_PUSH && (G1 - G2) > (uint64_t)(g.n / 4);
+        const bool lazy = !PARENTS && dir == BLEST_DIR_PUSH && (G1 - G2) > (uint64_t)(g.n / 2);
         if (dir == BLEST_DIR_PUSH) {
             const uint32_t total = U1 - U2;
             const bool precheck = total > (ALIGNED ? 64u : 2048u);  // level larger than ~2k tiles
