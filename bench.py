@@ -996,9 +996,12 @@ def run_reference(args, rank, world):
     import oracle as O
     if not O.ref_available():
         return {"impl": "reference", "unavailable": "oracle/_ref/libblest_ref.so was not built (no reference sources)"}
+    kind, gen, order, window, nsrc, desc = WORKLOADS[args.workload]
+    if kind in ("mbfs", "mbfs_multi", "serving"):
+        return {"impl": "reference", "unavailable": "the reference has no multi-source BFS or serving implementation "
+                                                    "(MBFS/BVSSMBFSKernel.cuh is empty; no server)"}
     import torch
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    kind, gen, order, window, nsrc, desc = WORKLOADS[args.workload]
     csc, bvss, csr, sources = prepare(args.workload, Path(args.cache), 0, 1)
     n = csc.n
     deg = np.diff(csr.col_ptrs.astype(np.int64))
