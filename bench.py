@@ -952,7 +952,7 @@ def run_cc(args, rank, world):
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "e2e": {"value": round(float(e2e_t.item()), 4), "unit": "ms", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 4 * n},
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": 4 * args.steps,  # init, queue seed, persistent propagation, component count
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_source": peak_kind, "traffic": None,
                      "algorithmic_bytes_per_launch": algo, "avg_launch_ms": round(kern_s * 1e3, 4)},

@@ -430,8 +430,8 @@ int blest_workspace_trace(blest_workspace* ws, blest_level_trace* out, uint32_t 
         blest::require(ws && out && count, "null argument");
         BLEST_CUDA(cudaSetDevice(ws->g->device));
         // BFS: one record per level + the end record; MBFS counts its own
-        const uint32_t its = ws->w.host_counters->iterations;
-        const uint32_t levels = its ? its : ws->w.host_counters->levels + 1;
+        const uint32_t recs = ws->w.host_counters->trace_records;
+        const uint32_t levels = recs ? recs : ws->w.host_counters->levels + 1;
         const uint32_t k = std::min<uint32_t>(std::min<uint32_t>(levels, max), BLEST_TRACE_CAPACITY);
         BLEST_CUDA(cudaMemcpy(out, ws->w.trace, sizeof(blest_level_trace) * k, cudaMemcpyDeviceToHost));
         *count = k;

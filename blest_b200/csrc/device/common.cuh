@@ -60,8 +60,9 @@ struct RunCounters {
     unsigned int levels;            // last level with discoveries
     unsigned int push_levels;
     unsigned int pull_levels;
-    unsigned int iterations;
-    unsigned int pad[7];
+    unsigned int iterations;        // CC: label-propagation iterations
+    unsigned int trace_records;     // multi-source BFS: level records written (0: BFS counts by levels)
+    unsigned int pad[6];
     // Slots reused across levels/iterations (queue counters, heavy-list
     // counters, trace maxima); each kernel documents its own use.
     unsigned long long aux[8];

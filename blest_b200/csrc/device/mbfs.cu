@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(512, 2) mbfs_persistent_kernel(MbfsArgs a) {
         for (uint32_t level = 1;; ++level) {
             const uint32_t slot = (level - 1) & 1;  // queue/counts produced by the previous sweep
             const uint64_t nf = ld_relaxed64(&c->aux[4 + slot]);
-            if (a.trace && tid == 0 && c->iterations < BLEST_TRACE_CAPACITY) {
+            if (a.trace && tid == 0 && c->trace_records < BLEST_TRACE_CAPACITY) {
                 // direction summary: 1 push, 2 pull, 3 both (several graphs)
                 uint32_t dirs = 0;
                 for (uint32_t p = 0; p < a.nparts && dirs != 3; ++p) {
@@ -336,7 +336,7 @@ __global__ void __launch_bounds__(512, 2) mbfs_persistent_kernel(MbfsArgs a) {
                     const uint32_t x = __ldcg(&a.part_nf[slot * a.nparts + p]);
                     if (x) dirs |= (double)x > (double)P.n * a.pull_fraction ? 2u : 1u;
                 }
-                blest_level_trace& t = a.trace[c->iterations++];
+                blest_level_trace& t = a.trace[c->trace_records++];
                 t.start_ns = global_ns();
                 t.level = nf ? level : 0;
                 t.direction = dirs;
