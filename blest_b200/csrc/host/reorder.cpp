@@ -77,8 +77,8 @@ std::vector<uint32_t> order_jaccard_window(const Csc& g, uint32_t slice_size, ui
         const uint32_t W = std::min(window, n);
         std::vector<uint8_t> cmark(W);
         std::vector<uint32_t> inter(W, 0);
-        std::vector<uint32_t> touched;
-        touched.reserve(W);
+        std::vector<uint32_t> touched(W);
+        uint32_t tsize = 0;
         std::vector<uint32_t> queue(W);
         std::vector<uint32_t> byDeg(W);
         std::vector<uint32_t> rmark(n, 0);
@@ -110,22 +110,26 @@ std::vector<uint32_t> order_jaccard_window(const Csc& g, uint32_t slice_size, ui
             auto scanRow = [&](uint32_t r) {
                 const uint32_t* b = ids + ptrs[r];
                 const uint32_t* e = ids + ptrs[r + 1];
+                // Branch-free: the placed/first-touch tests are unpredictable,
+                // so every column is written at the queue end and the end
+                // only advances for a first touch (same queue order).
                 for (const uint32_t* p = std::lower_bound(b, e, ws); p < e; ++p) {
                     const uint32_t c = *p;
                     if (c >= we) break;
-                    if (!cmark[c - ws]) {
-                        if (inter[c - ws] == 0) {
-                            queue[qsize++] = c;
-                            touched.push_back(c - ws);
-                        }
-                        ++inter[c - ws];
-                    }
+                    const uint32_t x = c - ws;
+                    const uint32_t unplaced = cmark[x] ^ 1u;
+                    const uint32_t first = unplaced & (uint32_t)(inter[x] == 0);
+                    queue[qsize] = c;
+                    qsize += first;
+                    touched[tsize] = x;
+                    tsize += first;
+                    inter[x] += unplaced;
                 }
             };
             const uint32_t noSets = (len + slice_size - 1) / slice_size;
             for (uint32_t s = 0; s < noSets; ++s) {
-                for (uint32_t x : touched) inter[x] = 0;
-                touched.clear();
+                for (uint32_t i = 0; i < tsize; ++i) inter[touched[i]] = 0;
+                tsize = 0;
                 qsize = 0;
                 const uint32_t sliceStart = ws + s * slice_size;
                 const uint32_t sliceEnd = std::min(sliceStart + slice_size, we);
