@@ -57,3 +57,54 @@ def test_null_arguments_are_rejected():
     assert L.fn["blest_csc_view_get"](None, None) == L.ERR_INVALID_ARG
     lab = np.zeros(3, dtype=np.uint32)
     assert L.fn["blest_cc_relabel_dense"](lab.ctypes.data_as(L.P(L.u32)), 3, None, None) == L.ERR_INVALID_ARG
+
+
+def test_documented_host_programs_compile_and_link(tmp_path):
+    """A C++ driver on the plugin classes (the reference's Benchmark flow)
+    and a C program on the multi-graph plan API, as a user of the library
+    writes them, compile against include/ and link against the library."""
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    inc, libdir = root / "include", root / "blest_b200"
+    cpp = tmp_path / "driver.cpp"
+    cpp.write_text('''
+#include <vector>
+#include "blest_kernels.hpp"
+int main() {
+    blest_csc* csc = nullptr;
+    if (blest_csc_read_mtx_auto("graph.mtx", &csc) != BLEST_OK) return 1;
+    blest_csc_view v;
+    blest_csc_view_get(csc, &v);
+    blest_order_params op{BLEST_ORDER_AUTO, 1, 65536, 0, 1, 0};
+    std::vector<uint32_t> inv(v.n);
+    blest_csc_reorder(csc, &op, inv.data());
+    blest_bvss* bvss = nullptr;
+    blest_bvss_build(csc, -1, &bvss);
+    blest_init(0);
+    blest_b200::DeviceGraph graph(bvss, csc);
+    blest_b200::B200BFSKernel kernel(&graph);
+    blest_b200::BFSResult r = kernel.run(inv[0]);
+    delete[] r.levels;
+    return 0;
+}
+''')
+    c = tmp_path / "plan.c"
+    c.write_text('''
+#include "blest.h"
+int main(void) {
+    blest_mbfs_item items[1] = {{0, 0, 0, 0}};
+    blest_mbfs_params mp = {32, 0, 0, 0.0625, 0};
+    blest_mbfs_plan* plan = 0;
+    blest_mbfs_stats st;
+    blest_mbfs_plan_info info;
+    if (blest_mbfs_plan_create(items, 1, &mp, 0, &plan) != BLEST_OK) return 1;
+    blest_mbfs_plan_info_get(plan, &info);
+    blest_mbfs_plan_run(plan, &st);
+    blest_mbfs_plan_destroy(plan);
+    return 0;
+}
+''')
+    for cmd in (["g++", "-std=c++17", f"-I{inc}", str(cpp), f"-L{libdir}", "-lblest_b200", "-o", str(tmp_path / "d")],
+                ["gcc", "-std=c11", f"-I{inc}", str(c), f"-L{libdir}", "-lblest_b200", "-o", str(tmp_path / "p")]):
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
