@@ -206,15 +206,42 @@ def measured_peak() -> tuple[float, str]:
 
 
 def profiled_traffic(workload: str):
-    """DRAM bytes per launch of the BFS kernel from the committed ncu summary
-    (profiles/bfs_<workload>_traffic.md, line 'traffic_bytes_per_launch: X')."""
-    p = ROOT / "profiles" / f"bfs_{workload}_traffic.md"
+    """DRAM bytes (read + write) per launch of the workload's dominant kernel
+    from one ncu capture, as recorded in profiles/traffic.json (a figure
+    scaled from a smaller capture says so in that file); None if absent."""
+    p = ROOT / "profiles" / "traffic.json"
     if not p.exists():
         return None
-    for line in p.read_text().splitlines():
-        if line.startswith("traffic_bytes_per_launch:"):
-            return float(line.split(":", 1)[1])
-    return None
+    entry = json.loads(p.read_text()).get(workload)
+    return float(entry["bytes_per_launch"]) if entry else None
+
+
+def bfs_config(workload, n, nnz, nsrc, edges_per_step, slices, world):
+    """Workload keys of a BFS line, the same for both arms."""
+    return {"workload": workload, "description": WORKLOADS[workload][5], "n": int(n), "nnz_directed": int(nnz),
+            "undirected_edges": int(nnz) // 2, "sources_per_step": int(nsrc),
+            "reached_edges_per_step": int(edges_per_step), "bvss_slices": int(slices),
+            "l2": "inputs larger than L2 (BVSS+CSR in HBM), no flush",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+
+
+def cc_config(workload, n, nnz, slices, components, world):
+    return {"workload": workload, "description": WORKLOADS[workload][5], "n": int(n), "nnz_directed": int(nnz),
+            "bvss_slices": int(slices), "components": int(components),
+            "l2": "inputs larger than L2 (BVSS in HBM), no flush",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+
+
+def generate_oracle(gen):
+    """The workload's graph from the oracle's generator (byte-identical to
+    the library's), as (n, col_ptrs, rows)."""
+    import oracle as O
+    if gen[0] == "rmat":
+        return O.gen_rmat(gen[1], gen[2], 0.57, 0.19, 0.19, SEED, SEED)
+    if gen[0] == "grid":
+        return O.gen_grid(gen[1], gen[2], 0.05, 0.001, SEED, 0)
+    n = 1 << gen[1]
+    return O.gen_er(n, n * gen[2] // 2, SEED, 0)
 
 
 # ----------------------------------------------------------------- arms
@@ -746,7 +773,7 @@ def run_b200(args, rank, world):
     import torch
     import torch.distributed as dist
     import blest_b200
-    from blest_b200 import Graph, Workspace
+    from blest_b200 import Graph, Workspace, bfs_params
     from blest_b200._lib import MEM_HOST
 
     dev = int(os.environ.get("LOCAL_RANK", "0"))
@@ -764,7 +791,7 @@ def run_b200(args, rank, world):
     out = torch.empty(n, dtype=torch.int32, device="cuda")
     barrier = (lambda: dist.barrier()) if world > 1 else (lambda: None)
 
-    params = None
+    params = bfs_params("auto", args.slice_test)
     tuned = None
     if args.autotune:
         from blest_b200.autotune import tune_bfs
@@ -772,22 +799,33 @@ def run_b200(args, rank, world):
         tuned = table[0]["params"]
         log(f"[autotune] best {tuned}: {table[0]['seconds'] * 1e3:.3f} ms/BFS "
             f"(worst {table[-1]['seconds'] * 1e3:.3f})")
-    # Reference answers for m_R (levels are deterministic), outside timing.
+    # Outside timing: every source once -- reached edges and algorithmic
+    # bytes from its levels, and (rank 0) parity of the levels with the
+    # oracle's OpenMP BFS on the host cores, whose run times are also the
+    # CPU baseline.
     host_lv = np.empty(n, dtype=np.uint32)
     mr, algo = [], []
     arrays = bvss.arrays()
+    check = rank == 0 and not args.skip_check
+    parity = {"sources_checked": 0, "mismatches": 0, "against": "oracle bfs_omp (oracle/oracle.c), all sources"}
+    cpu_secs, cpu_edges, cpu_used = 0.0, 0, 0
+    if check:
+        import oracle as O
     for s in sources:
-        ws.bfs(int(s), host_lv, sptr)
+        ws.bfs(int(s), host_lv, sptr, params=params)
         mr.append(reached_edges(deg, host_lv))
         algo.append(algorithmic_bytes(arrays, host_lv))
-    # correctness guard on two sources against the CPU oracle (outside timing)
-    if rank == 0 and not args.skip_check:
-        import oracle as O
-        for s in sources[:2]:
-            ws.bfs(int(s), host_lv, sptr)
-            want = O.bfs_csc(n, csc.col_ptrs, csc.rows, int(s))
+        if check:
+            t = time.perf_counter()
+            want, cpu_used = O.bfs_omp(n, csc.col_ptrs, csc.rows, csr.col_ptrs, csr.rows, int(s), 0)
+            cpu_secs += time.perf_counter() - t
+            cpu_edges += mr[-1]
+            parity["sources_checked"] += 1
             if not np.array_equal(host_lv, want):
-                raise SystemExit(f"BFS levels differ from the oracle for source {s}")
+                parity["mismatches"] += 1
+                log(f"[parity] source {int(s)}: {int((host_lv != want).sum())} levels differ from the oracle")
+    if parity["mismatches"]:
+        raise SystemExit(f"BFS levels differ from the oracle for {parity['mismatches']} of {len(sources)} sources")
     edges_per_step = sum(mr)
 
     def step(events=None):
@@ -798,8 +836,14 @@ def run_b200(args, rank, world):
             if events is not None:
                 events[i][1].record(stream)
 
+    def settle(count):
+        # settle the oldest `count` calls (every call's record is checked)
+        for _ in range(count):
+            ws.sync_one()
+
     for _ in range(args.warmup):
         step()
+        settle(len(sources))
     stream.synchronize()
     per_bfs = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                 for _ in sources] for _ in range(args.steps)]
@@ -810,8 +854,11 @@ def run_b200(args, rank, world):
         t0.record(stream)
         for k in range(args.steps):
             step(per_bfs[k])
+            if k:
+                settle(len(sources))  # step k - 1 (step k keeps the GPU busy)
         t1.record(stream)
         stream.synchronize()
+    ws.sync()
     barrier()
     torch.cuda.synchronize()
     ms = t0.elapsed_time(t1)
@@ -822,18 +869,42 @@ def run_b200(args, rank, world):
     ms = float(ms_t.item())
     value = edges_per_step * args.steps * world / (ms * 1e-3) / 1e9
 
-    # e2e: public API, host (pinned) output, copy inside the timed region
-    pinned = torch.empty(n, dtype=torch.int32, pin_memory=True)
-    pin_np = pinned.numpy().view(np.uint32)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    for s in sources[: min(4, len(sources))]:
-        ws.bfs(int(s), pin_np, sptr)
-    barrier()
-    torch.cuda.synchronize()
-    e0.record(stream)
+    # The same BFS calls timed by the reference's convention (host wall
+    # clock from launch to synchronisation, one BFS at a time;
+    # BFS/BVSSBFSKernel.cuh:1469,1545-1548).
+    wall = 0.0
     for _ in range(args.steps):
         for s in sources:
-            ws.bfs(int(s), pin_np, sptr, params=params)
+            t = time.perf_counter()
+            ws.bfs_async(int(s), out.data_ptr(), sptr, params=params)
+            ws.sync()
+            wall += time.perf_counter() - t
+    wall_t = torch.tensor([wall], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(wall_t, op=dist.ReduceOp.MAX)
+    value_wall = edges_per_step * args.steps * world / float(wall_t.item()) / 1e9
+
+    # e2e: the public call with pinned HOST output, copies inside the timed
+    # region; the pipelined mode overlaps the copy of BFS i with the kernel
+    # of BFS i + 1 (two host buffers, call i settled after call i + 1 is
+    # issued).
+    bufs = [torch.empty(n, dtype=torch.int32, pin_memory=True) for _ in range(2)]
+    bptr = [b.data_ptr() for b in bufs]
+    for i, s in enumerate(sources[: min(4, len(sources))]):
+        ws.bfs_async(int(s), bptr[i % 2], sptr, out_mem=MEM_HOST, params=params)
+        ws.sync()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    j = 0
+    for _ in range(args.steps):
+        for s in sources:
+            ws.bfs_async(int(s), bptr[j % 2], sptr, out_mem=MEM_HOST, params=params)
+            if j:
+                ws.sync_one()
+            j += 1
+    ws.sync_one()
     e1.record(stream)
     stream.synchronize()
     e2e_ms_t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
@@ -841,7 +912,30 @@ def run_b200(args, rank, world):
         dist.all_reduce(e2e_ms_t, op=dist.ReduceOp.MAX)
     e2e_ms = float(e2e_ms_t.item())
     e2e = edges_per_step * args.steps * world / (e2e_ms * 1e-3) / 1e9
+    if check:
+        # the last pipelined result must still equal the oracle's
+        last = sources[-1]
+        want, _ = O.bfs_omp(n, csc.col_ptrs, csc.rows, csr.col_ptrs, csr.rows, int(last), 0)
+        if not np.array_equal(bufs[(j - 1) % 2].numpy().view(np.uint32), want):
+            raise SystemExit("pipelined host-output BFS differs from the oracle")
 
+    if args.trace_levels and rank == 0:
+        # per-level records of a few traced BFS runs (diagnostics, stderr)
+        from blest_b200 import _lib as L
+        import ctypes as C
+        tp = bfs_params("auto", args.slice_test, trace=True)
+        recs = (L.LevelTrace * 4096)()
+        for s in sources[: args.trace_levels]:
+            ws.bfs_async(int(s), out.data_ptr(), sptr, params=tp)
+            st = ws.sync()
+            cnt = L.u32()
+            L.call("blest_workspace_trace", ws._h, recs, 4096, C.byref(cnt))
+            log(f"[trace] source {int(s)}: {cnt.value - 1} levels, {st.time * 1e3:.3f} ms "
+                f"(push {st.push_levels}, pull {st.pull_levels})")
+            for i in range(cnt.value - 1):
+                r, nx = recs[i], recs[i + 1]
+                log(f"[trace]   L{r.level:<4d} {'push' if r.direction == 1 else 'pull'} frontier {r.frontier:>9d} "
+                    f"units {r.work_units:>10d} {(nx.start_ns - r.start_ns) / 1e3:9.1f} us")
     peak, peak_kind = measured_peak()
     avg_bytes = float(np.mean(algo))
     avg_launch_s = float(np.mean(bfs_ms)) * 1e-3
@@ -852,25 +946,29 @@ def run_b200(args, rank, world):
         "value": round(value, 3), "unit": "GTEPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generator; see config)",
-        "config": {"workload": args.workload, "description": desc, "n": n, "nnz_directed": csc.nnz,
-                   "undirected_edges": csc.nnz // 2, "sources_per_step": int(len(sources)),
-                   "reached_edges_per_step": edges_per_step, "bvss_slices": int(info.no_slices),
-                   "graph_bytes_hbm": int(info.device_bytes_graph),
-                   "l2": "inputs larger than L2 (BVSS+CSR in HBM), no flush",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "bfs_params": tuned or "defaults (alpha 14, beta 24, occupancy grid, CUDA-core slice test)"},
+        "config": bfs_config(args.workload, n, csc.nnz, len(sources), edges_per_step, info.no_slices, world),
+        "impl_detail": {"bfs_params": tuned or f"defaults (alpha 14, beta 24, occupancy grid, "
+                                                 f"{args.slice_test} slice test)",
+                        "graph_bytes_hbm": int(info.device_bytes_graph)},
+        "value_reference_timing": {"value": round(value_wall, 3), "unit": "GTEPS",
+                                   "note": "host wall time launch -> synchronise per BFS, the reference's "
+                                           "convention (BFS/BVSSBFSKernel.cuh:1469,1545-1548)"},
         "e2e": {"value": round(e2e, 3), "unit": "GTEPS", "h2d_bytes_per_step": 4 * int(len(sources)),
-                "d2h_bytes_per_step": 4 * n * int(len(sources))},
+                "d2h_bytes_per_step": 4 * n * int(len(sources)),
+                "note": "blest_bfs_ws with pinned host output, copy of BFS i overlapped with BFS i + 1"},
         "gpu_launches": int(len(sources)) * args.steps,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                      "traffic": traffic, "algorithmic_bytes_per_launch": int(avg_bytes),
                      "avg_launch_ms": round(avg_launch_s * 1e3, 4)},
     }
-    clk = clocks.summary()
-    result["clocks"] = clk
-    if rank == 0 and not args.no_cpu_baseline:
-        result["cpu_baseline"] = cpu_baseline(csc, csr, sources, deg, args)
+    if check:
+        result["parity"] = parity
+    result["clocks"] = clocks.summary()
+    if check and not args.no_cpu_baseline:
+        result["cpu_baseline"] = {"value": round(cpu_edges / cpu_secs / 1e9, 4), "unit": "GTEPS", "cores": cpu_used,
+                                  "kind": "port", "sample": f"{len(sources)} of {len(sources)} sources "
+                                                            f"(the parity runs), {cpu_secs:.1f} s"}
     return result
 
 
@@ -898,10 +996,14 @@ def run_cc(args, rank, world):
     sptr = stream.cuda_stream
     out = torch.empty(n, dtype=torch.int32, device="cuda")
     lab, st0 = g.cc()
+    parity = None
     if rank == 0 and not args.skip_check:
         import oracle as O
-        if not np.array_equal(lab, O.cc_csc(n, csc.col_ptrs, csc.rows)):
-            raise SystemExit("CC labels differ from the oracle")
+        bad = int((lab != O.cc_csc(n, csc.col_ptrs, csc.rows)).sum())
+        parity = {"runs_checked": 1, "mismatches": int(bad > 0), "labels_differing": bad,
+                  "against": "oracle cc_csc (union-find fixpoint: minimum vertex id per component)"}
+        if bad:
+            raise SystemExit(f"CC labels differ from the oracle at {bad} vertices")
     for _ in range(args.warmup):
         ws.cc(out.data_ptr(), sptr)
     kern = []
@@ -945,11 +1047,8 @@ def run_cc(args, rank, world):
         "value": round(ms, 4), "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms, 4), "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generator; see config)",
-        "config": {"workload": args.workload, "description": desc, "n": n, "nnz_directed": csc.nnz,
-                   "bvss_slices": int(info.no_slices), "iterations": int(st0.iterations),
-                   "components": int(st0.no_components),
-                   "l2": "inputs larger than L2 (BVSS in HBM), no flush",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "config": cc_config(args.workload, n, csc.nnz, info.no_slices, st0.no_components, world),
+        "impl_detail": {"iterations": int(st0.iterations)},
         "e2e": {"value": round(float(e2e_t.item()), 4), "unit": "ms", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 4 * n},
         "gpu_launches": 4 * args.steps,  # init, queue seed, persistent propagation, component count
@@ -958,6 +1057,8 @@ def run_cc(args, rank, world):
                      "algorithmic_bytes_per_launch": algo, "avg_launch_ms": round(kern_s * 1e3, 4)},
         "clocks": clocks.summary(),
     }
+    if parity:
+        result["parity"] = parity
     if rank == 0 and not args.no_cpu_baseline:
         # the oracle's OpenMP CC on all host cores, the whole graph once
         import oracle as O
@@ -969,29 +1070,43 @@ def run_cc(args, rank, world):
     return result
 
 
-def cpu_baseline(csc, csr, sources, deg, args):
-    """OpenMP direction-optimising BFS (the oracle's CPU baseline) on the
-    host cores, over a bounded sample of the sources (~10-30 s)."""
+def prepare_reference(workload: str):
+    """The workload's graph built by the REFERENCE's own host code through
+    oracle/_ref (never libblest_b200.so): the oracle generator's CSC (the
+    same bytes as the library's generator), the reference's CSC object and
+    classification, its ordering (Jaccard window or RCM), its BVSS builder
+    with FULL_PADDING = !social (Benchmark.cuh:113-114, 187-194), and the
+    seeded sources mapped to the new ids as Benchmark.cuh:80 does."""
     import oracle as O
-    n = csc.n
-    t_ptrs, t_ids = csr.col_ptrs, csr.rows
-    edges, secs, used, done = 0, 0.0, 0, 0
-    budget = args.cpu_budget
-    for s in sources:
-        t = time.perf_counter()
-        lv, used = O.bfs_omp(n, csc.col_ptrs, csc.rows, t_ptrs, t_ids, int(s), 0)
-        secs += time.perf_counter() - t
-        edges += reached_edges(deg, lv)
-        done += 1
-        if secs > budget:
-            break
-    return {"value": round(edges / secs / 1e9, 4), "unit": "GTEPS", "cores": used, "kind": "port",
-            "sample": f"{done} of {len(sources)} sources, {secs:.1f} s"}
+    kind, gen, order, window, nsrc, _ = WORKLOADS[workload]
+    t0 = time.time()
+    n, cp, rw = generate_oracle(gen)
+    src = O.sample_sources(n, cp, nsrc, SEED) if nsrc else np.zeros(0, np.uint32)
+    t1 = time.time()
+    ref = O.RefGraph.from_csc(n, cp, rw)
+    del cp, rw
+    social = ref.is_social()
+    inv = ref.reorder(order, window or 65536)
+    t2 = time.time()
+    ref.build_bvss(full_padding=not social)
+    t3 = time.time()
+    _, nnz, rcp, rrw = ref.csc()
+    slices = int(ref.bvss_slices())
+    log(f"[prep:reference] {workload}: generate {t1 - t0:.1f}s reorder {t2 - t1:.1f}s bvss {t3 - t2:.1f}s "
+        f"n={n} nnz={nnz} social={social} slices={slices}")
+    return ref, n, nnz, rcp, rrw, inv[src] if len(src) else src, slices
 
 
 def run_reference(args, rank, world):
-    """The reference's BVSSBFSKernel::hostCode (kernels compiled from the
-    reference's sources for sm_100a) on the identical BVSS; rank 0 only."""
+    """The reference's own stock path, independent of this library: its
+    host code builds the graph (prepare_reference) and
+    BVSSBFSKernel::hostCode / BVSSCCKernel::hostCode (its kernels compiled
+    from its sources for sm_100a, oracle/_ref) run it, each call uploading
+    the graph and downloading the result as the reference does
+    (BFS/BVSSBFSKernel.cuh:1385-1447, 1550). `value` is the reference's own
+    timing (launch -> cudaDeviceSynchronize); `e2e` is the wall time of the
+    whole hostCode call. Each timed step is a bounded sample of the
+    workload's sources (rotating, so all of them are covered); rank 0 only."""
     if rank != 0:
         return None
     import oracle as O
@@ -1001,62 +1116,114 @@ def run_reference(args, rank, world):
     if kind in ("mbfs", "mbfs_multi", "serving"):
         return {"impl": "reference", "unavailable": "the reference has no multi-source BFS or serving implementation "
                                                     "(MBFS/BVSSMBFSKernel.cuh is empty; no server)"}
-    import torch
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    csc, bvss, csr, sources = prepare(args.workload, Path(args.cache), 0, 1)
-    n = csc.n
-    deg = np.diff(csr.col_ptrs.astype(np.int64))
-    ref = O.RefGraph.from_bvss(n, bvss.arrays(), bvss.full_padding, bvss.update_divergence, csr.col_ptrs, csr.rows)
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    ref, n, nnz, cp, rw, sources, slices = prepare_reference(args.workload)
+    deg = np.diff(cp.astype(np.int64))
+    variant = ["BVSSBFS8EnhancedSliceSize8NoMasks4", "FullPad", "LazySwitching", "LazyFullPad"][ref.bfs_variant()]
     if kind == "cc":
-        for _ in range(args.warmup):
-            ref.cc_raw(n)
-        with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
-            ts = [ref.cc_raw(n)[1] for _ in range(args.steps)]
+        t = time.perf_counter()
+        comp, secs0, k0 = ref.cc(n)
+        wall0 = time.perf_counter() - t
+        parity = None
+        if not args.skip_check:
+            # the reference's host relabel scrambles labels (CC/BVSSCCKernel.cuh:1282-1287): compare the
+            # component count with the oracle's
+            want = O.cc_csc(n, cp, rw)
+            k_want = int(np.unique(want).size)
+            parity = {"runs_checked": 1, "mismatches": int(k0 != k_want), "components": int(k0),
+                      "against": "oracle cc_csc component count (the reference's relabelled labels are not a "
+                                 "partition, CC/BVSSCCKernel.cuh:1282-1287)"}
+        for _ in range(args.warmup - 1):
+            ref.cc(n)
+        ts, walls = [], []
+        with ClockSampler(dev) as clocks:
+            for _ in range(args.steps):
+                t = time.perf_counter()
+                ts.append(ref.cc(n)[1])
+                walls.append(time.perf_counter() - t)
         ms = float(np.mean(ts)) * 1e3
-        return {
+        res = {
             "impl": "reference", "metric": "CC time (BVSS label propagation, labels = component minimum id)",
             "value": round(ms, 4), "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(ms, 4), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "u32", "data": "synthetic (seeded generator; see config)",
-            "config": {"workload": args.workload, "description": desc, "n": n,
-                       "timing": "reference convention: launch -> cudaDeviceSynchronize around the label "
-                                 "propagation kernels (CC/BVSSCCKernel.cuh), graph upload untimed"},
-            "cpu_baseline": {"value": round(ms, 4), "unit": "ms", "cores": 0, "kind": "reference",
-                             "sample": f"{args.steps} runs on the GPU (the reference's CC kernels built for sm_100a)"},
-            "e2e": {"value": round(ms, 4), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "config": cc_config(args.workload, n, nnz, slices, k0, 1),
+            "impl_detail": {"reference_kernel": "BVSSCC8EnhancedSliceSize8NoMasks4" +
+                            ("LazyFullPad" if variant.endswith("FullPad") else "Lazy"),
+                            "timing": "BVSSCCKernel::hostCode's own time (launch -> cudaDeviceSynchronize)"},
+            "e2e": {"value": round(float(np.mean(walls)) * 1e3, 4), "unit": "ms",
+                    "h2d_bytes_per_step": None, "d2h_bytes_per_step": 4 * n,
+                    "note": "wall time of the whole stock hostCode call: per-call graph upload, run, label download, "
+                            "host relabel"},
             "clocks": clocks.summary(),
         }
-    sample = sources[: args.ref_sources]
-    variant = ["BVSSBFS8EnhancedSliceSize8NoMasks4", "FullPad", "LazySwitching", "LazyFullPad"][ref.bfs_variant()]
+        if parity:
+            res["parity"] = parity
+        if not args.no_cpu_baseline:
+            t = time.perf_counter()
+            _, used = O.cc_omp(n, cp, rw)
+            secs = time.perf_counter() - t
+            res["cpu_baseline"] = {"value": round(secs * 1e3, 2), "unit": "ms", "cores": int(used), "kind": "port",
+                                   "sample": f"the oracle's OpenMP CC, the whole graph once, {secs:.1f} s (the "
+                                             f"reference has no CPU path)"}
+        return res
+
+    # Every source once: reached edges, parity against the oracle (the
+    # oracle's OpenMP BFS on the host cores, whose times are the CPU
+    # baseline), and the first warm-up step.
     mr = {}
-    for _ in range(args.warmup):
-        for s in sample[:2]:
-            ref.bfs(int(s), n)
-    tot_t, tot_e = 0.0, 0
-    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+    parity = {"sources_checked": 0, "mismatches": 0, "against": "oracle bfs_omp (oracle/oracle.c), all sources"}
+    cpu_secs, cpu_edges, cpu_used = 0.0, 0, 0
+    for s in sources:
+        lv, _, _, _ = ref.bfs(int(s), n)
+        mr[int(s)] = reached_edges(deg, lv)
+        if not args.skip_check:
+            t = time.perf_counter()
+            want, cpu_used = O.bfs_omp(n, cp, rw, cp, rw, int(s), 0)
+            cpu_secs += time.perf_counter() - t
+            cpu_edges += mr[int(s)]
+            parity["sources_checked"] += 1
+            parity["mismatches"] += int(not np.array_equal(lv, want))
+    per_step = max(1, min(args.ref_sources, len(sources)))
+    for _ in range(args.warmup - 1):
+        ref.bfs(int(sources[0]), n)
+    tot_t, tot_wall, tot_e, k = 0.0, 0.0, 0, 0
+    with ClockSampler(dev) as clocks:
         for _ in range(args.steps):
-            for s in sample:
-                lv, t, _, _ = ref.bfs(int(s), n)
-                if int(s) not in mr:
-                    mr[int(s)] = reached_edges(deg, lv)
-                tot_t += t
-                tot_e += mr[int(s)]
+            for _ in range(per_step):
+                s = int(sources[k % len(sources)])
+                k += 1
+                t = time.perf_counter()
+                _, secs, _, _ = ref.bfs(s, n)
+                tot_wall += time.perf_counter() - t
+                tot_t += secs
+                tot_e += mr[s]
     value = tot_e / tot_t / 1e9
-    return {
+    res = {
         "impl": "reference", "metric": "BFS GTEPS (single-source, direction-optimising BVSS BFS)",
         "value": round(value, 3), "unit": "GTEPS", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(tot_t * 1e3 / args.steps, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generator; see config)",
-        "config": {"workload": args.workload, "description": desc, "n": n, "sources_per_step": int(len(sample)),
-                   "reference_kernel": variant,
-                   "timing": "reference convention: omp_get_wtime launch -> cudaDeviceSynchronize "
-                             "(BFS/BVSSBFSKernel.cuh:1469,1545-1548); graph upload per call untimed"},
-        "cpu_baseline": {"value": round(value, 3), "unit": "GTEPS", "cores": 0, "kind": "reference",
-                         "sample": f"{len(sample)} sources x {args.steps} steps on the GPU (the reference has "
-                                   f"no CPU BFS; its BVSS kernels built for sm_100a)"},
-        "e2e": {"value": round(value, 3), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "config": bfs_config(args.workload, n, nnz, len(sources), sum(mr.values()), slices, 1),
+        "impl_detail": {"reference_kernel": variant,
+                        "timing": "BVSSBFSKernel::hostCode's own time: omp_get_wtime launch -> cudaDeviceSynchronize "
+                                  "(BFS/BVSSBFSKernel.cuh:1469,1545-1548)"},
+        "sample": f"{per_step} of the {len(sources)} sources per timed step, rotating ({k} BFS calls); every source "
+                  f"ran once before timing",
+        "e2e": {"value": round(tot_e / tot_wall / 1e9, 4), "unit": "GTEPS",
+                "h2d_bytes_per_step": None, "d2h_bytes_per_step": 4 * n * per_step,
+                "note": "wall time of the whole stock hostCode call: per-call graph upload "
+                        "(BFS/BVSSBFSKernel.cuh:1385-1447), run, level download (:1550)"},
         "clocks": clocks.summary(),
     }
+    if not args.skip_check:
+        res["parity"] = parity
+        if not args.no_cpu_baseline:
+            res["cpu_baseline"] = {"value": round(cpu_edges / cpu_secs / 1e9, 4), "unit": "GTEPS",
+                                   "cores": cpu_used, "kind": "port",
+                                   "sample": f"the oracle's OpenMP BFS on all {len(sources)} sources, "
+                                             f"{cpu_secs:.1f} s (the reference has no CPU BFS)"}
+    return res
 
 
 def main():
@@ -1067,8 +1234,10 @@ def main():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="rmat24")
     ap.add_argument("--cache", default="/tmp/blest_bench_cache")
-    ap.add_argument("--ref-sources", type=int, default=64)
-    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--ref-sources", type=int, default=8,
+                    help="reference arm: sources per timed step (each call re-uploads the graph)")
+    ap.add_argument("--slice-test", choices=["cuda_core", "mma"], default="cuda_core",
+                    help="BFS slice test: CUDA-core byte AND, or the b1 mma.sync m8n8k128 AND+POPC")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-check", action="store_true")
     ap.add_argument("--group-width", type=int, default=128)
@@ -1079,6 +1248,8 @@ def main():
     ap.add_argument("--serving-full", action="store_true")
     ap.add_argument("--buffers", type=int, default=192)
     ap.add_argument("--autotune", action="store_true", help="tune BFS launch parameters before timing")
+    ap.add_argument("--trace-levels", type=int, default=0,
+                    help="BFS: log per-level timings of this many traced runs to stderr")
     ap.add_argument("--no-autotune-mbfs", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -184,9 +184,11 @@ _SIGS = {
     "blest_bfs": [vp, u32, vp, vp, i32, P(BfsParams), P(BfsStats)],
     "blest_bfs_ws": [vp, u32, vp, vp, i32, P(BfsParams), vp, i32, P(BfsStats)],
     "blest_workspace_sync": [vp, P(BfsStats)],
+    "blest_workspace_sync_one": [vp, P(i32), P(BfsStats)],
     "blest_workspace_trace": [vp, P(LevelTrace), u32, P(u32)],
     "blest_graph_default_workspace": [vp, P(vp)],
     "blest_bfs_noalloc": [P(DeviceGraphView), u32, vp, vp, vp, P(BfsStats)],
+    "blest_selftest_barrier": [u32, u32, u64, u32, P(f64)],
     "blest_cc": [vp, vp, i32, P(CcStats)],
     "blest_cc_ws": [vp, vp, i32, vp, P(CcStats)],
     "blest_cc_relabel_dense": [P(u32), u32, P(u32), P(u32)],

@@ -4,7 +4,10 @@
 #include <omp.h>
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cstring>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -145,6 +148,10 @@ void workspace_alloc(const blest_graph* g, Workspace& w) {
     w.heavy_cap = g->d.nnz / 1024 + 64;
     alloc((void**)&w.heavy, sizeof(uint4) * w.heavy_cap);
     BLEST_CUDA(cudaMallocHost((void**)&w.host_counters, sizeof(dev::RunCounters)));
+    BLEST_CUDA(cudaHostAlloc((void**)&w.records, sizeof(dev::RunRecord) * kRecordRing, cudaHostAllocMapped));
+    // no slot may look like a finished call before its kernel wrote it
+    std::memset((void*)w.records, 0xFF, sizeof(dev::RunRecord) * kRecordRing);
+    w.call_slot = new int8_t[kRecordRing];
     BLEST_CUDA(cudaEventCreate(&w.ev_start));
     BLEST_CUDA(cudaEventCreate(&w.ev_stop));
 }
@@ -162,6 +169,10 @@ void workspace_free(Workspace& w) {
     for (auto& x : w.summary) cudaFree(x);
     cudaFree(w.heavy);
     mbfs_scratch_free(w.mbfs);
+    if (w.records) cudaFreeHost(w.records);
+    delete[] w.call_slot;
+    cudaFree(w.levels_b);
+    cudaFree(w.parents_b);
     if (w.host_counters) cudaFreeHost(w.host_counters);
     if (w.ev_start) cudaEventDestroy(w.ev_start);
     if (w.ev_stop) cudaEventDestroy(w.ev_stop);
@@ -194,20 +205,103 @@ blest_bfs_params default_bfs_params() {
     return p;
 }
 
-void fill_bfs_stats(const blest::Workspace& w, uint32_t src, float ms, blest_bfs_stats* st) {
-    const blest::dev::RunCounters& c = *w.host_counters;
-    if (c.error) throw blest::Error((int)c.error, c.error == BLEST_ERR_BARRIER_TIMEOUT
-                                                      ? "device grid barrier timed out"
-                                                      : (c.error == BLEST_ERR_LEVEL_CAP ? "BFS exceeded n + 1 levels"
-                                                                                         : "device reported an out-of-range index"));
+const char* bfs_error_text(uint32_t code) {
+    return code == BLEST_ERR_BARRIER_TIMEOUT ? "device grid barrier timed out"
+           : code == BLEST_ERR_LEVEL_CAP     ? "BFS exceeded n + 1 levels"
+                                             : "device reported an out-of-range index";
+}
+
+// Pipelined host output: the copy stream, its events and the second pair
+// of internal buffers, created on the first such call.
+void ensure_pipeline(blest_workspace* ws) {
+    if (ws->copy_stream) return;
+    blest::Workspace& w = ws->w;
+    const uint32_t n = ws->g->d.n;
+    BLEST_CUDA(cudaMalloc((void**)&w.levels_b, 4ull * n));
+    BLEST_CUDA(cudaMalloc((void**)&w.parents_b, 4ull * n));
+    w.bytes += 8ull * n;
+    for (int i = 0; i < 2; ++i) {
+        BLEST_CUDA(cudaEventCreateWithFlags(&ws->ev_kernel[i], cudaEventDisableTiming));
+        BLEST_CUDA(cudaEventCreateWithFlags(&ws->ev_copy[i], cudaEventDisableTiming));
+    }
+    BLEST_CUDA(cudaStreamCreateWithFlags(&ws->copy_stream, cudaStreamNonBlocking));
+}
+
+void release_pipeline(blest_workspace* ws) {
+    if (ws->copy_stream) {
+        cudaStreamSynchronize(ws->copy_stream);
+        cudaStreamDestroy(ws->copy_stream);
+    }
+    for (int i = 0; i < 2; ++i) {
+        if (ws->ev_kernel[i]) cudaEventDestroy(ws->ev_kernel[i]);
+        if (ws->ev_copy[i]) cudaEventDestroy(ws->ev_copy[i]);
+    }
+}
+
+// Settle the oldest BFS call issued on `ws` and not yet checked: wait
+// until it is done (its host copy, for a pipelined call; the stream
+// otherwise), read its record and report its failure. `st` gets its
+// counts and its kernel's device time.
+void finish_one(blest_workspace* ws, blest_bfs_stats* st) {
+    blest::Workspace& w = ws->w;
+    const uint64_t seq = ws->synced++;
+    const int slot = w.call_slot[seq % blest::kRecordRing];
+    if (ws->issued - seq > blest::kRecordRing) {
+        // its record was overwritten: settle the rest first, then report
+        ws->synced = ws->issued - blest::kRecordRing;
+        throw blest::Error(BLEST_ERR_INVALID_ARG, std::to_string(ws->synced - seq) +
+                                                      " asynchronous BFS calls were not checked (more than " +
+                                                      std::to_string(blest::kRecordRing) +
+                                                      " issued without blest_workspace_sync)");
+    }
+    if (slot >= 0 && ws->slot_busy[slot]) {
+        // ev_copy[slot] is this call's copy or a later one's on the same
+        // slot; either way the slot's last copy is then done
+        BLEST_CUDA(cudaEventSynchronize(ws->ev_copy[slot]));
+        ws->slot_busy[slot] = false;
+    } else if (slot < 0) {
+        // Wait for this call's record only (later calls keep running): its
+        // kernel writes seq last, after a system-scope fence. If the stream
+        // has drained and the record is still missing, the call failed.
+        const volatile unsigned long long* vs = &w.records[seq % blest::kRecordRing].seq;
+        for (uint32_t spin = 0; *vs != seq; ++spin) {
+            const cudaError_t q = cudaStreamQuery(ws->stream);
+            if (q == cudaSuccess) break;
+            if (q != cudaErrorNotReady) BLEST_CUDA(q);
+            if (spin > 64) std::this_thread::sleep_for(std::chrono::microseconds(20));
+        }
+        std::atomic_thread_fence(std::memory_order_acquire);
+    }
+    const blest::dev::RunRecord& r = w.records[seq % blest::kRecordRing];
+    if (r.seq != seq) throw blest::Error(BLEST_ERR_CUDA, "BFS call " + std::to_string(seq) + " left no record");
+    if (r.error) throw blest::Error((int)r.error, bfs_error_text(r.error));
     if (!st) return;
-    st->time = ms * 1e-3;
-    st->source_vertex = src;
-    st->total_levels = c.levels;
-    st->no_visited = (uint32_t)c.discovered;
-    st->push_levels = c.push_levels;
-    st->pull_levels = c.pull_levels;
-    st->reached_degree_sum = c.degree;
+    st->time = (double)(r.end_ns - r.start_ns) * 1e-9;
+    st->source_vertex = r.source;
+    st->total_levels = r.levels;
+    st->no_visited = (uint32_t)r.discovered;
+    st->push_levels = r.push_levels;
+    st->pull_levels = r.pull_levels;
+    st->reached_degree_sum = r.degree;
+}
+
+// Settle every pending call; the first failure is reported after all of
+// them are settled, `st` gets the last call's outcome.
+void finish_pending(blest_workspace* ws, blest_bfs_stats* st) {
+    int code = BLEST_OK;
+    std::string msg;
+    while (ws->synced < ws->issued) {
+        const bool last = ws->synced + 1 == ws->issued;
+        try {
+            finish_one(ws, last ? st : nullptr);
+        } catch (const blest::Error& e) {
+            if (code == BLEST_OK) {
+                code = e.code;
+                msg = e.what();
+            }
+        }
+    }
+    if (code != BLEST_OK) throw blest::Error(code, msg);
 }
 
 }  // namespace
@@ -309,6 +403,7 @@ int blest_graph_destroy(blest_graph* g) {
     cudaSetDevice(g->device);
     if (g->stream) cudaStreamSynchronize(g->stream);
     if (g->default_ws) {
+        release_pipeline(g->default_ws);
         blest::workspace_free(g->default_ws->w);
         delete g->default_ws;
     }
@@ -367,6 +462,7 @@ int blest_workspace_set_grid(blest_workspace* ws, uint32_t blocks) {
 int blest_workspace_destroy(blest_workspace* ws) {
     if (!ws) return BLEST_OK;
     cudaSetDevice(ws->g->device);
+    release_pipeline(ws);
     blest::workspace_free(ws->w);
     delete ws;
     return BLEST_OK;
@@ -385,43 +481,61 @@ int blest_bfs_ws(blest_workspace* ws, uint32_t source, uint32_t* levels_out, uin
         blest::require(p.slice_test == BLEST_TEST_CUDA_CORE || p.slice_test == BLEST_TEST_B1_MMA, "bad slice_test");
         cudaStream_t s = stream ? (cudaStream_t)stream : (ws->stream ? ws->stream : g->stream);
         blest::Workspace& w = ws->w;
-        uint32_t* dl = out_mem == BLEST_MEM_DEVICE ? levels_out : w.levels;
-        uint32_t* dp = parents_out ? (out_mem == BLEST_MEM_DEVICE ? parents_out : w.parents) : nullptr;
-        BLEST_CUDA(cudaEventRecord(w.ev_start, s));
-        blest::launch_bfs(g, w, source, dl, dp, p, s);
-        BLEST_CUDA(cudaEventRecord(w.ev_stop, s));
-        // the run's status is copied back here only for a blocking call; an
-        // asynchronous one reads it in blest_workspace_sync
-        if (!async)
-            BLEST_CUDA(cudaMemcpyAsync(w.host_counters, w.counters, sizeof(blest::dev::RunCounters),
-                                       cudaMemcpyDeviceToHost, s));
+        // a blocking call first settles the asynchronous ones before it
+        if (!async) finish_pending(ws, nullptr);
+        const uint64_t seq = ws->issued;
+        const bool pipelined = async && out_mem == BLEST_MEM_HOST;
+        const int slot = pipelined ? (int)(seq & 1) : 0;
+        if (pipelined) {
+            ensure_pipeline(ws);
+            // the slot's previous copy (call seq - 2) must be done before
+            // this kernel overwrites the slot
+            if (ws->slot_busy[slot]) {
+                BLEST_CUDA(cudaEventSynchronize(ws->ev_copy[slot]));
+                ws->slot_busy[slot] = false;
+            }
+        }
+        uint32_t* hl = slot ? w.levels_b : w.levels;
+        uint32_t* hp = slot ? w.parents_b : w.parents;
+        uint32_t* dl = out_mem == BLEST_MEM_DEVICE ? levels_out : hl;
+        uint32_t* dp = parents_out ? (out_mem == BLEST_MEM_DEVICE ? parents_out : hp) : nullptr;
+        w.call_slot[seq % blest::kRecordRing] = (int8_t)(pipelined ? slot : -1);
+        blest::launch_bfs(g, w, source, dl, dp, p, s, seq);
+        ws->issued = seq + 1;
+        ws->stream = s;
+        if (pipelined) {
+            BLEST_CUDA(cudaEventRecord(ws->ev_kernel[slot], s));
+            BLEST_CUDA(cudaStreamWaitEvent(ws->copy_stream, ws->ev_kernel[slot], 0));
+            BLEST_CUDA(cudaMemcpyAsync(levels_out, dl, 4ull * g->d.n, cudaMemcpyDeviceToHost, ws->copy_stream));
+            if (parents_out)
+                BLEST_CUDA(cudaMemcpyAsync(parents_out, dp, 4ull * g->d.n, cudaMemcpyDeviceToHost, ws->copy_stream));
+            BLEST_CUDA(cudaEventRecord(ws->ev_copy[slot], ws->copy_stream));
+            ws->slot_busy[slot] = true;
+            return;
+        }
         if (out_mem == BLEST_MEM_HOST) {
             BLEST_CUDA(cudaMemcpyAsync(levels_out, dl, 4ull * g->d.n, cudaMemcpyDeviceToHost, s));
             if (parents_out) BLEST_CUDA(cudaMemcpyAsync(parents_out, dp, 4ull * g->d.n, cudaMemcpyDeviceToHost, s));
         }
-        ws->pending = true;
-        ws->pending_src = source;
-        ws->stream = s;
         if (async) return;
-        BLEST_CUDA(cudaStreamSynchronize(s));
-        ws->pending = false;
-        float ms = 0;
-        BLEST_CUDA(cudaEventElapsedTime(&ms, w.ev_start, w.ev_stop));
-        fill_bfs_stats(w, source, ms, stats);
+        finish_pending(ws, stats);
     });
 }
 
 int blest_workspace_sync(blest_workspace* ws, blest_bfs_stats* stats) {
     return guarded([&] {
         blest::require(ws, "null argument");
-        if (!ws->pending) return;
-        BLEST_CUDA(cudaStreamSynchronize(ws->stream));
-        ws->pending = false;
-        BLEST_CUDA(cudaMemcpy(ws->w.host_counters, ws->w.counters, sizeof(blest::dev::RunCounters),
-                              cudaMemcpyDeviceToHost));
-        float ms = 0;
-        BLEST_CUDA(cudaEventElapsedTime(&ms, ws->w.ev_start, ws->w.ev_stop));
-        fill_bfs_stats(ws->w, ws->pending_src, ms, stats);
+        BLEST_CUDA(cudaSetDevice(ws->g->device));
+        finish_pending(ws, stats);
+    });
+}
+
+int blest_workspace_sync_one(blest_workspace* ws, int* settled, blest_bfs_stats* stats) {
+    return guarded([&] {
+        blest::require(ws, "null argument");
+        BLEST_CUDA(cudaSetDevice(ws->g->device));
+        if (settled) *settled = ws->synced < ws->issued ? 1 : 0;
+        if (ws->synced < ws->issued) finish_one(ws, stats);
     });
 }
 
@@ -429,9 +543,12 @@ int blest_workspace_trace(blest_workspace* ws, blest_level_trace* out, uint32_t 
     return guarded([&] {
         blest::require(ws && out && count, "null argument");
         BLEST_CUDA(cudaSetDevice(ws->g->device));
-        // BFS: one record per level + the end record; MBFS counts its own
-        const uint32_t recs = ws->w.host_counters->trace_records;
-        const uint32_t levels = recs ? recs : ws->w.host_counters->levels + 1;
+        // BFS: one record per level + the end record; MBFS counts its own.
+        // The counters of the last run are still on the device.
+        blest::dev::RunCounters c;
+        BLEST_CUDA(cudaMemcpy(&c, ws->w.counters, sizeof(c), cudaMemcpyDeviceToHost));
+        const uint32_t recs = c.trace_records;
+        const uint32_t levels = recs ? recs : c.levels + 1;
         const uint32_t k = std::min<uint32_t>(std::min<uint32_t>(levels, max), BLEST_TRACE_CAPACITY);
         BLEST_CUDA(cudaMemcpy(out, ws->w.trace, sizeof(blest_level_trace) * k, cudaMemcpyDeviceToHost));
         *count = k;

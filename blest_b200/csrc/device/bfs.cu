@@ -64,6 +64,10 @@ struct BfsArgs {
     uint4* heavy;
     uint32_t heavy_cap;
     uint32_t heavy_min;
+    // Where the run's outcome goes (null: nowhere) and the call number it
+    // carries.
+    RunRecord* record;
+    uint64_t seq;
 };
 
 __device__ __forceinline__ uint32_t* summary_buf(const BfsArgs& a, uint32_t level) {
@@ -372,7 +376,7 @@ __device__ __forceinline__ void add_level_counts(unsigned long long* lvl, uint32
 }
 
 template <bool ALIGNED, bool MMA, bool PARENTS>
-__global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(BfsArgs a) {
+__device__ __forceinline__ void bfs_run(const BfsArgs& a) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t nth = gridDim.x * blockDim.x;
@@ -780,6 +784,31 @@ __global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(BfsArgs a) {
     }
 }
 
+// The BFS, then (block 0, thread 0, on every exit path) the run's record:
+// thread 0 of block 0 wrote the counts itself, and an error recorded by any
+// block was visible to it at the barrier that ended its run.
+template <bool ALIGNED, bool MMA, bool PARENTS>
+__global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(BfsArgs a) {
+    const uint64_t t0 = global_ns();
+    bfs_run<ALIGNED, MMA, PARENTS>(a);
+    if (a.record && blockIdx.x == 0 && threadIdx.x == 0) {
+        const RunCounters* c = a.ctr;
+        RunRecord* r = a.record;
+        r->start_ns = t0;
+        r->end_ns = global_ns();
+        r->error = ld_relaxed(&c->error);
+        r->discovered = c->discovered;
+        r->degree = c->degree;
+        r->levels = c->levels;
+        r->push_levels = c->push_levels;
+        r->pull_levels = c->pull_levels;
+        r->source = a.src;
+        // the host polls seq: it must become visible after the rest
+        __threadfence_system();
+        *(volatile unsigned long long*)&r->seq = a.seq;
+    }
+}
+
 }  // namespace dev
 
 namespace {
@@ -819,8 +848,10 @@ void launch_variant(const blest_graph* g, const dev::BfsArgs& args, int blocks_p
 }  // namespace
 
 void launch_bfs(const blest_graph* g, Workspace& w, uint32_t src, uint32_t* levels, uint32_t* parents,
-                const blest_bfs_params& p, cudaStream_t s) {
+                const blest_bfs_params& p, cudaStream_t s, uint64_t seq) {
     dev::BfsArgs a{};
+    a.record = w.records ? &w.records[seq % kRecordRing] : nullptr;
+    a.seq = seq;
     a.g = g->d;
     a.levels = levels;
     a.parents = parents;
@@ -938,9 +969,33 @@ extern "C" int blest_bfs_noalloc(const blest_device_graph_view* g, uint32_t sour
         int device = 0;
         BLEST_CUDA(cudaGetDevice(&device));
         require(device >= 0 && device < kNoAllocMaxDevices, "device ordinal out of range");
+        // The scratch array and the launch belong to the current device, so
+        // the caller's stream and buffers must too.
+        if (stream) {
+            int sdev = -1;
+            BLEST_CUDA(cudaStreamGetDevice((cudaStream_t)stream, &sdev));
+            if (sdev != device) throw Error(BLEST_ERR_INVALID_ARG, "stream belongs to another device than the current one");
+        }
+        auto on_device = [&](const void* p, const char* what) {
+            cudaPointerAttributes at{};
+            BLEST_CUDA(cudaPointerGetAttributes(&at, p));
+            if (!((at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) && at.device == device))
+                throw Error(BLEST_ERR_INVALID_ARG, std::string(what) + " is not memory of the current device");
+        };
+        on_device(levels_out, "levels_out");
+        if (parents_out) on_device(parents_out, "parents_out");
+        on_device(g->slice_set_ptrs, "slice_set_ptrs");
+        on_device(g->real_ptrs, "real_ptrs");
+        on_device(g->csr_ptrs, "csr_ptrs");
+        if (g->no_slices) {
+            on_device(g->row_ids, "row_ids");
+            on_device(g->masks, "masks");
+        }
+        if (g->nnz) on_device(g->csr_ids, "csr_ids");
         std::lock_guard<std::mutex> lock(g_noalloc_mutex[device]);
         // One-time set-up per device (this device current): the device
-        // address of the scratch array.
+        // address of the scratch array, kept for the life of the process
+        // (not valid after a cudaDeviceReset, which the header rules out).
         if (!g_noalloc_ptr[device]) {
             void* p = nullptr;
             BLEST_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));

@@ -77,6 +77,25 @@ struct RunCounters {
     unsigned long long pad_arrive[15];
 };
 
+// Outcome of one single-source BFS launch, written by the kernel itself as
+// its last act into a ring of the workspace (slot = call number % ring
+// size), so that asynchronous calls issued back to back each leave their
+// status and counts for blest_workspace_sync to check.
+struct RunRecord {
+    unsigned long long seq;         // call number (checked by the reader)
+    unsigned long long discovered;  // vertices reached
+    unsigned long long degree;      // their degree sum
+    unsigned long long start_ns;    // %globaltimer at block 0's start and end
+    unsigned long long end_ns;
+    unsigned int error;
+    unsigned int levels;            // max level + 1
+    unsigned int push_levels;
+    unsigned int pull_levels;
+    unsigned int source;
+    unsigned int pad;
+};
+static_assert(sizeof(RunRecord) == 64, "RunRecord is one 64-byte slot");
+
 __device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
     uint32_t v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -115,27 +134,31 @@ __device__ __forceinline__ uint64_t ld_acquire64(const unsigned long long* p) {
 // the next barrier reports it to every block without an extra load.
 __device__ __forceinline__ void set_error(RunCounters* c, uint32_t code) {
     atomicCAS(&c->error, 0u, code);
+    __threadfence();  // the code is visible to whoever sees the flag
     atomicOr(&c->arrive, kArriveError);
 }
 
 // Thread 0's half of the grid barrier: arrive and wait. The arrival count
 // only grows (one per block per barrier), so the k-th barrier is complete
-// when it reaches k * gridDim.x; the value the atomic returns says which k
+// when it reaches k * `expected` (the number of blocks that take part,
+// gridDim.x in every kernel); the value the atomic returns says which k
 // this block is at, so no generation word has to be read or reset, and the
 // last block to arrive leaves at once. The wait is bounded: a block that
-// waits longer than kBarrierTimeoutNs records BLEST_ERR_BARRIER_TIMEOUT and
-// leaves. Returns the final counter value (bit 63 = error recorded).
-__device__ __forceinline__ uint64_t barrier_arrive_wait(RunCounters* c) {
+// waits longer than `timeout_ns` records BLEST_ERR_BARRIER_TIMEOUT and
+// leaves, and a block that sees another block's error flag leaves too, so
+// one timed-out block ends the wait of all the others. Returns the final
+// counter value (bit 63 = error recorded).
+__device__ __forceinline__ uint64_t barrier_arrive_wait(RunCounters* c, uint64_t expected, uint64_t timeout_ns) {
     __threadfence();
-    const uint64_t n = gridDim.x;
     uint64_t v = atomicAdd(&c->arrive, 1ull);
-    const uint64_t target = ((v & ~kArriveError) / n + 1) * n;
+    const uint64_t target = ((v & ~kArriveError) / expected + 1) * expected;
     ++v;
-    if ((v & ~kArriveError) < target) {
+    if ((v & ~kArriveError) < target && !(v & kArriveError)) {
         const uint64_t t0 = global_ns();
         uint32_t spins = 0;
         while (((v = ld_acquire64(&c->arrive)) & ~kArriveError) < target) {
-            if ((++spins & 31) == 0 && global_ns() - t0 > kBarrierTimeoutNs) {
+            if (v & kArriveError) return v;
+            if ((++spins & 31) == 0 && global_ns() - t0 > timeout_ns) {
                 set_error(c, BLEST_ERR_BARRIER_TIMEOUT);
                 return kArriveError;
             }
@@ -146,16 +169,22 @@ __device__ __forceinline__ uint64_t barrier_arrive_wait(RunCounters* c) {
     return v;
 }
 
+__device__ __forceinline__ uint64_t barrier_arrive_wait(RunCounters* c) {
+    return barrier_arrive_wait(c, gridDim.x, kBarrierTimeoutNs);
+}
+
 // Grid-wide barrier for a cooperative (co-resident) launch. Returns false
 // if the run has an error recorded (every caller then returns), so no wait
 // is unbounded.
-__device__ __forceinline__ bool grid_barrier(RunCounters* c) {
+__device__ __forceinline__ bool grid_barrier(RunCounters* c, uint64_t expected, uint64_t timeout_ns) {
     __shared__ uint32_t s_ok;
     __syncthreads();
-    if (threadIdx.x == 0) s_ok = (barrier_arrive_wait(c) & kArriveError) == 0;
+    if (threadIdx.x == 0) s_ok = (barrier_arrive_wait(c, expected, timeout_ns) & kArriveError) == 0;
     __syncthreads();
     return s_ok;
 }
+
+__device__ __forceinline__ bool grid_barrier(RunCounters* c) { return grid_barrier(c, gridDim.x, kBarrierTimeoutNs); }
 
 // Warp-inclusive scan of a 64-bit value.
 __device__ __forceinline__ uint64_t warp_inclusive_scan64(uint64_t v) {

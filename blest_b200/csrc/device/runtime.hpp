@@ -41,8 +41,22 @@ struct Workspace {
     uint32_t grid_blocks = 0;                   // cap on cooperative grid size (0 = whole GPU)
     void* mbfs = nullptr;                       // multi-source BFS scratch (mbfs.cu), grown on demand
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    // Outcome of every single-source BFS call, slot = call number %
+    // kRecordRing: mapped pinned host memory that the kernel writes
+    // directly, so reading a finished call's record needs no copy.
+    dev::RunRecord* records = nullptr;
+    // Pipelined slot (0/1) of each call, or -1 (same ring positions).
+    int8_t* call_slot = nullptr;
+    // Second level/parent buffers of the pipelined host-output mode (the
+    // first pair is `levels`/`parents`), allocated on first use.
+    uint32_t* levels_b = nullptr;
+    uint32_t* parents_b = nullptr;
     uint64_t bytes = 0;
 };
+
+// Asynchronous BFS calls whose outcome a workspace keeps until
+// blest_workspace_sync reads it.
+constexpr uint32_t kRecordRing = BLEST_BFS_RECORD_RING;
 
 }  // namespace blest
 
@@ -61,12 +75,20 @@ struct blest_graph {
 struct blest_workspace {
     const blest_graph* g = nullptr;
     blest::Workspace w;
-    // async bookkeeping
+    // Asynchronous bookkeeping: BFS calls are numbered; calls [synced,
+    // issued) have not been checked yet. `stream` is the last call's.
     cudaStream_t stream = nullptr;
-    uint32_t pending_src = 0;
-    bool pending = false;
-    uint32_t* pending_levels_host = nullptr;
-    uint32_t* pending_parents_host = nullptr;
+    uint64_t issued = 0;
+    uint64_t synced = 0;
+    // Pipelined host output: the kernel of call i writes slot i % 2 of the
+    // internal buffers on the call's stream; the slot's copy to the
+    // caller's host buffer runs on copy_stream, so it overlaps the next
+    // call's kernel. ev_kernel/ev_copy order the two; slot_busy: the slot's
+    // copy was issued and not yet waited for.
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_kernel[2] = {nullptr, nullptr};
+    cudaEvent_t ev_copy[2] = {nullptr, nullptr};
+    bool slot_busy[2] = {false, false};
 };
 
 namespace blest {
@@ -84,8 +106,10 @@ inline uint32_t heavy_threshold(uint32_t nnz, uint32_t cap) {
 void workspace_free(Workspace& w);
 
 // Kernel launchers (bfs.cu, cc.cu). Outputs are device pointers.
+// `seq`: call number; the kernel writes its outcome to
+// w.records[seq % kRecordRing].
 void launch_bfs(const blest_graph* g, Workspace& w, uint32_t src, uint32_t* levels, uint32_t* parents,
-                const blest_bfs_params& p, cudaStream_t s);
+                const blest_bfs_params& p, cudaStream_t s, uint64_t seq);
 void launch_cc(const blest_graph* g, Workspace& w, uint32_t* labels, cudaStream_t s);
 
 int device_sm_count(int device);

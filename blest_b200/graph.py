@@ -405,13 +405,27 @@ class Workspace:
 
     def bfs_async(self, source: int, levels_ptr: int, stream: int, parents_ptr: int | None = None,
                   params: L.BfsParams | None = None, out_mem: int = L.MEM_DEVICE) -> None:
-        """Enqueue a BFS on `stream` (a cudaStream_t as int); returns at once."""
+        """Enqueue a BFS on `stream` (a cudaStream_t as int); returns at once.
+        With out_mem=MEM_HOST (a pinned buffer that must stay untouched until
+        the call is settled) the copy overlaps the next call's kernel."""
         L.call("blest_bfs_ws", self._h, source, levels_ptr, parents_ptr, out_mem,
                C.byref(params) if params is not None else None, stream, 1, None)
 
     def sync(self) -> BfsStats:
+        """Settle every pending asynchronous call (first failure raised);
+        returns the last call's stats."""
         st = L.BfsStats()
         L.call("blest_workspace_sync", self._h, C.byref(st))
+        return BfsStats(st.time, st.source_vertex, st.total_levels, st.no_visited, st.push_levels,
+                        st.pull_levels, st.reached_degree_sum)
+
+    def sync_one(self) -> BfsStats | None:
+        """Settle the oldest pending call only (None when nothing is pending)."""
+        st = L.BfsStats()
+        done = L.i32()
+        L.call("blest_workspace_sync_one", self._h, C.byref(done), C.byref(st))
+        if not done.value:
+            return None
         return BfsStats(st.time, st.source_vertex, st.total_levels, st.no_visited, st.push_levels,
                         st.pull_levels, st.reached_degree_sum)
 

@@ -271,10 +271,28 @@ typedef struct blest_bfs_stats {
 int blest_bfs(blest_graph* g, uint32_t source, uint32_t* levels_out, uint32_t* parents_out, int out_mem,
               const blest_bfs_params* params, blest_bfs_stats* stats);
 /* Same on an explicit workspace and stream; returns when the work is
- * enqueued if `async` != 0 (stats then filled by blest_workspace_sync). */
+ * enqueued if `async` != 0. Every call is numbered and its kernel leaves
+ * its outcome in a ring of BLEST_BFS_RECORD_RING records on the workspace;
+ * blest_workspace_sync / _sync_one check them (more calls than the ring
+ * between two syncs are reported as unchecked). Asynchronous calls on one
+ * workspace must use one stream (they share its buffers).
+ * Asynchronous host output (out_mem BLEST_MEM_HOST, async != 0) is
+ * pipelined: the kernel writes one of two internal buffers and the copy to
+ * `levels_out` (pinned memory, for the copy to be asynchronous) runs on a
+ * copy stream of the workspace, so it overlaps the next call's kernel;
+ * `levels_out` must stay valid and untouched until the call is settled. A
+ * blocking call (async == 0) first settles every pending one. */
 int blest_bfs_ws(blest_workspace* ws, uint32_t source, uint32_t* levels_out, uint32_t* parents_out, int out_mem,
                  const blest_bfs_params* params, void* stream, int async, blest_bfs_stats* stats);
+#define BLEST_BFS_RECORD_RING 1024
+/* Settle every pending asynchronous call on `ws`: wait for it (and its host
+ * copy), check its record; returns the first failure among them, stats =
+ * the last call's outcome (time = its kernel's device time). */
 int blest_workspace_sync(blest_workspace* ws, blest_bfs_stats* stats);
+/* Settle only the oldest pending call (so later calls keep running and
+ * copying); *settled = 0 when nothing was pending. For a pipelined loop:
+ * issue call i, then settle call i - 1, whose host buffer is then ready. */
+int blest_workspace_sync_one(blest_workspace* ws, int* settled, blest_bfs_stats* stats);
 /* Level records of the last traced BFS (or multi-source BFS: one record per
  * level of every group, direction 1 push / 2 pull / 3 both) on `ws`. */
 int blest_workspace_trace(blest_workspace* ws, blest_level_trace* out, uint32_t max, uint32_t* count);
@@ -294,13 +312,19 @@ int blest_graph_default_workspace(blest_graph* g, blest_workspace** out);
  * are rejected with BLEST_ERR_UNSUPPORTED. The caller passes the graph
  * (a valid BVSS and its pull CSR, e.g. as built by blest_bvss_build and
  * blest_csc_transpose, copied into its own device memory) and device
- * output buffers. The first call on a device looks up the scratch array's
- * device address (with that device current); make that first call before
- * any stream capture. All calls on a device share the one scratch array,
- * so calls whose GPU work overlapped would race: this function serialises
- * callers per device and returns only when its work on `stream` is done.
- * Levels (and parents, if non-NULL) are identical to blest_bfs's; stats
- * time is host wall time of the call. */
+ * output buffers, all on the current device; the stream, the graph arrays
+ * and the outputs must belong to that device (BLEST_ERR_INVALID_ARG
+ * otherwise). The first call on a device looks up the scratch array's
+ * device address (with that device current) and keeps it for the life of
+ * the process; make that first call before any stream capture, and do not
+ * call this function again on a device after cudaDeviceReset. All calls on
+ * a device share the one scratch array, which keeps the last call's
+ * contents (every call re-initialises what it reads); calls whose GPU work
+ * overlapped would race, so this function serialises callers per device
+ * and always synchronises `stream` before it returns. Levels are identical
+ * to blest_bfs's; parents, if non-NULL, form a valid BFS tree (which
+ * parent is recorded may differ from blest_bfs's, whose pull lists are
+ * re-ordered at upload). stats time is host wall time of the call. */
 #define BLEST_NOALLOC_MAX_VERTICES (1u << 20)
 typedef struct blest_device_graph_view {
     uint32_t n;
@@ -316,6 +340,20 @@ typedef struct blest_device_graph_view {
 } blest_device_graph_view;
 int blest_bfs_noalloc(const blest_device_graph_view* g, uint32_t source, uint32_t* levels_out,
                       uint32_t* parents_out, void* stream, blest_bfs_stats* stats);
+
+/* ---- diagnostics ---------------------------------------------------------
+ * No counterpart in the reference (its grid.sync() waits without a bound,
+ * BFS/BVSSBFSKernel.cuh:204-283). Runs the bounded grid barrier that every
+ * persistent kernel here ends its levels with, `rounds` times, in a
+ * cooperative launch of `blocks` blocks of 128 threads on the current
+ * device, telling it to expect blocks + missing_blocks arrivals and to give
+ * up a wait after timeout_ns. With missing_blocks = 0 every round completes
+ * and the call returns BLEST_OK; otherwise no round can complete, every
+ * block's wait runs out (or sees another block's timeout) and the call
+ * returns BLEST_ERR_BARRIER_TIMEOUT, with the device still usable.
+ * *seconds (may be NULL) = host wall time from launch to completion. */
+int blest_selftest_barrier(uint32_t blocks, uint32_t missing_blocks, uint64_t timeout_ns, uint32_t rounds,
+                           double* seconds);
 
 /* ---- connected components ------------------------------------------------ */
 /* Mirrors CCResult (CC/CCKernel.cuh:21-26). */

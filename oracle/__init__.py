@@ -50,6 +50,10 @@ def _p64(a: np.ndarray):
 _olib = None
 
 
+class OracleGraph(C.Structure):
+    _fields_ = [("n", C.c_uint32), ("nnz", C.c_uint64), ("col_ptrs", P32), ("rows", P32)]
+
+
 def olib():
     global _olib
     if _olib is None:
@@ -66,6 +70,16 @@ def olib():
         lib.oracle_cc_omp.argtypes = [C.c_uint32, P32, P32, P32, C.c_int]
         lib.oracle_reached_degree_sum.argtypes = [C.c_uint32, P32, P32]
         lib.oracle_reached_degree_sum.restype = C.c_uint64
+        for name, args in (("oracle_gen_rmat", [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double,
+                                                C.c_uint64, C.c_uint64, C.POINTER(OracleGraph)]),
+                           ("oracle_gen_grid", [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_uint64,
+                                                C.c_uint64, C.POINTER(OracleGraph)]),
+                           ("oracle_gen_er", [C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64,
+                                              C.POINTER(OracleGraph)])):
+            getattr(lib, name).argtypes = args
+        lib.oracle_graph_free.argtypes = [C.POINTER(OracleGraph)]
+        lib.oracle_graph_free.restype = None
+        lib.oracle_sample_sources.argtypes = [C.c_uint32, P32, C.c_uint32, C.c_uint64, P32, P32]
         _olib = lib
     return _olib
 
@@ -127,6 +141,39 @@ def cc_omp(n, col_ptrs, rows, threads=0):
     out = np.empty(n, dtype=np.uint32)
     used = olib().oracle_cc_omp(n, _p32(cp), _p32(rw), _p32(out), threads)
     return out, used
+
+
+def _take_graph(fn, *args):
+    g = OracleGraph()
+    rc = fn(*args, C.byref(g))
+    if rc != 0:
+        raise RuntimeError(f"oracle graph generator failed ({rc})")
+    try:
+        cp = np.ctypeslib.as_array(g.col_ptrs, shape=(g.n + 1,)).copy()
+        rw = np.ctypeslib.as_array(g.rows, shape=(max(g.nnz, 1),))[: g.nnz].copy()
+    finally:
+        olib().oracle_graph_free(C.byref(g))
+    return g.n, cp, rw
+
+
+def gen_rmat(scale, edge_factor, a=0.57, b=0.19, c=0.19, seed=1, permute_seed=0):
+    """(n, col_ptrs, rows) of the seeded RMAT graph blest_csc_generate_rmat makes."""
+    return _take_graph(olib().oracle_gen_rmat, scale, edge_factor, a, b, c, seed, permute_seed)
+
+
+def gen_grid(width, height, p_delete, shortcut_fraction, seed=1, permute_seed=0):
+    return _take_graph(olib().oracle_gen_grid, width, height, p_delete, shortcut_fraction, seed, permute_seed)
+
+
+def gen_er(n, m, seed=1, permute_seed=0):
+    return _take_graph(olib().oracle_gen_er, n, m, seed, permute_seed)
+
+
+def sample_sources(n, col_ptrs, k, seed) -> np.ndarray:
+    out = np.empty(max(k, 1), dtype=np.uint32)
+    cnt = C.c_uint32()
+    assert olib().oracle_sample_sources(n, _p32(_u32(col_ptrs)), k, seed, _p32(out), C.byref(cnt)) == 0
+    return out[: cnt.value].copy()
 
 
 def reached_degree_sum(n, col_ptrs, levels) -> int:
@@ -249,6 +296,16 @@ class RefGraph:
         return {"n": n.value, "update_divergence": div.value,
                 "slice_set_ptrs": arr(ssp, V.value + 1), "virtual_to_real": arr(v2r, V.value),
                 "real_ptrs": arr(rp, R.value + 1), "row_ids": arr(ri, S.value), "masks": arr(mk, S.value // 4)}
+
+    def bvss_slices(self) -> int:
+        """Slice count of the built BVSS (no array copies)."""
+        n, R, V = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        S = C.c_uint64()
+        div = C.c_double()
+        ssp, v2r, rp, ri, mk = P64(), P32(), P32(), P32(), P32()
+        _rcheck(rlib().ref_bvss_get(self.h, C.byref(n), C.byref(R), C.byref(V), C.byref(S), C.byref(div),
+                                    C.byref(ssp), C.byref(v2r), C.byref(rp), C.byref(ri), C.byref(mk)))
+        return S.value
 
     def bfs_variant(self) -> int:
         v = C.c_int()

@@ -69,6 +69,27 @@ int oracle_cc_omp(uint32_t n, const uint32_t* col_ptrs, const uint32_t* rows, ui
 /* Sum of out-degrees of the vertices with levels[v] != UNREACHED. */
 uint64_t oracle_reached_degree_sum(uint32_t n, const uint32_t* col_ptrs, const uint32_t* levels);
 
+/* Seeded synthetic graphs (gen.cpp): inputs for the reference arm of the
+ * benchmark, byte-identical to blest_csc_generate_rmat/_grid/_er with the
+ * same arguments. Symmetrised, de-duplicated, self-loop free CSC; arrays
+ * malloc'd, released by oracle_graph_free. Return 0 on success. */
+typedef struct oracle_graph {
+    uint32_t n;
+    uint64_t nnz;
+    uint32_t* col_ptrs;
+    uint32_t* rows;
+} oracle_graph;
+int oracle_gen_rmat(uint32_t scale, uint32_t edge_factor, double a, double b, double c, uint64_t seed,
+                    uint64_t permute_seed, oracle_graph* out);
+int oracle_gen_grid(uint32_t width, uint32_t height, double p_delete, double shortcut_fraction, uint64_t seed,
+                    uint64_t permute_seed, oracle_graph* out);
+int oracle_gen_er(uint32_t n, uint64_t m, uint64_t seed, uint64_t permute_seed, oracle_graph* out);
+void oracle_graph_free(oracle_graph* g);
+/* Seeded sample of k distinct vertices with degree >= 1, the same draw as
+ * blest_csc_sample_sources. */
+int oracle_sample_sources(uint32_t n, const uint32_t* col_ptrs, uint32_t k, uint64_t seed, uint32_t* out,
+                          uint32_t* count);
+
 #ifdef __cplusplus
 }
 #endif

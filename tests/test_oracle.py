@@ -103,3 +103,25 @@ def test_oracle_pinned_to_reference_kernels(path):
         np.testing.assert_array_equal(O.bfs_csc(n, h["reordered_col_ptrs"], h["reordered_rows"], int(s)), lv)
     if "cc_raw" in f:
         np.testing.assert_array_equal(O.cc_csc(n, h["reordered_col_ptrs"], h["reordered_rows"]), f["cc_raw"])
+
+
+@pytest.mark.parametrize("kind", ["rmat", "rmat_perm", "grid", "grid_perm", "er"])
+def test_oracle_generator_equals_the_library(kind):
+    """The reference arm of the benchmark builds its inputs with the oracle's
+    generator; they must be the library's graphs byte for byte."""
+    from blest_b200 import Csc
+    if kind.startswith("rmat"):
+        ps = 7 if kind == "rmat_perm" else 0
+        n, cp, rw = O.gen_rmat(11, 12, 0.57, 0.19, 0.19, 9, ps)
+        c = Csc.rmat(11, 12, 0.57, 0.19, 0.19, seed=9, permute_seed=ps)
+    elif kind.startswith("grid"):
+        ps = 3 if kind == "grid_perm" else 0
+        n, cp, rw = O.gen_grid(61, 29, 0.05, 0.01, 4, ps)
+        c = Csc.grid(61, 29, 0.05, 0.01, seed=4, permute_seed=ps)
+    else:
+        n, cp, rw = O.gen_er(3001, 20000, 5, 0)
+        c = Csc.er(3001, 20000, seed=5)
+    assert n == c.n
+    np.testing.assert_array_equal(cp, c.col_ptrs)
+    np.testing.assert_array_equal(rw, c.rows)
+    np.testing.assert_array_equal(O.sample_sources(n, cp, 40, 11), c.sample_sources(40, 11))

@@ -7,10 +7,14 @@ grow memory per call). Such a caller already holds the graph and the output
 buffers in its own device memory; here the test plays that caller, copies
 the graph to the GPU itself, and calls the entry point through the C ABI.
 
-Its levels and parents must equal the regular entry point's (blest_bfs) on
-consecutive calls that share the library's one scratch array; graphs above
-its vertex limit are refused before any GPU work. Integer results, so the
-tolerance is exact equality.
+Its levels must equal the oracle's and the regular entry point's
+(blest_bfs) on consecutive calls that share the library's one scratch
+array, including a graph at its vertex limit, a graph whose vertex count is
+not a multiple of 8 or 32, and a smaller graph run right after a larger one
+(whatever the larger left in the scratch must not leak into the result);
+parents must form a valid BFS tree. Graphs above its vertex limit and
+buffers that are not device memory are refused before any GPU work.
+Integer results, so the tolerance is exact equality.
 """
 import ctypes as C
 
@@ -64,6 +68,7 @@ def test_noalloc_equals_blest_bfs_on_consecutive_calls(gpu):
                stream.cuda_stream, C.byref(st))
         got = levels.cpu().numpy().view(np.uint32)
         np.testing.assert_array_equal(got, want)
+        np.testing.assert_array_equal(got, O.bfs_csc(n, csc.col_ptrs, csc.rows, s))
         par = parents.cpu().numpy().view(np.uint32)
         assert O.check_parents(n, csc.col_ptrs, csc.rows, s, got, par) == 0
         assert (st.no_visited, st.total_levels, st.reached_degree_sum) == \
@@ -83,3 +88,53 @@ def test_noalloc_refuses_graphs_over_its_limit(gpu):
         L.call("blest_bfs_noalloc", C.byref(view), 0, 256, None, None, None)
     assert e.value.code == L.ERR_UNSUPPORTED
     assert "at most" in str(e.value)
+
+
+def _prepared(kind):
+    if kind == "rmat20":
+        csc = Csc.rmat(20, 16, seed=23, permute_seed=5)
+        csc.reorder("jaccard", window=65536)
+    else:
+        csc = Csc.er(1001, 6000, seed=8)
+        csc.reorder("rcm")
+    return csc, Bvss.build(csc), csc.transpose()
+
+
+def test_noalloc_at_its_limit_and_after_a_larger_graph(gpu):
+    import torch
+    big, small = _prepared("rmat20"), _prepared("er1001")
+    assert big[0].n == L.NOALLOC_MAX_VERTICES and small[0].n % 8 != 0 and small[0].n % 32 != 0
+    stream = torch.cuda.Stream()
+    dev = {}
+    for name, (csc, bvss, csr) in (("big", big), ("small", small)):
+        view, keep = _device_graph(csc, bvss, csr)
+        out = torch.empty(csc.n, dtype=torch.int32, device="cuda")
+        par = torch.empty(csc.n, dtype=torch.int32, device="cuda")
+        src = [int(s) for s in csc.sample_sources(2, seed=31)]
+        dev[name] = (csc, view, keep, out, par, src)
+    # big, small, big, small: each call reuses the scratch the previous
+    # (differently sized) call left behind
+    for name, i in (("big", 0), ("small", 0), ("big", 1), ("small", 1)):
+        csc, view, keep, out, par, src = dev[name]
+        s = src[i]
+        st = L.BfsStats()
+        L.call("blest_bfs_noalloc", C.byref(view), s, out.data_ptr(), par.data_ptr(), stream.cuda_stream,
+               C.byref(st))
+        got = out.cpu().numpy().view(np.uint32)
+        want = O.bfs_csc(csc.n, csc.col_ptrs, csc.rows, s)
+        np.testing.assert_array_equal(got, want, err_msg=f"{name} source {s}")
+        assert O.check_parents(csc.n, csc.col_ptrs, csc.rows, s, got, par.cpu().numpy().view(np.uint32)) == 0
+        reached = want != O.UNREACHED
+        assert st.no_visited == int(reached.sum())
+        assert st.total_levels == int(want[reached].max()) + 1
+
+
+def test_noalloc_refuses_host_buffers(gpu):
+    csc, bvss, csr = _prepared("er1001")
+    view, keep = _device_graph(csc, bvss, csr)
+    host = np.empty(csc.n, dtype=np.uint32)
+    # a host (unregistered) output buffer is refused before any launch
+    with pytest.raises(BlestError) as e:
+        L.call("blest_bfs_noalloc", C.byref(view), 0, host.ctypes.data, None, None, None)
+    assert e.value.code == L.ERR_INVALID_ARG
+    assert "not memory of the current device" in str(e.value)
