@@ -174,8 +174,10 @@ _SIGS = {
     "blest_bvss_save_bin": [vp, C.c_char_p],
     "blest_bvss_load_bin": [C.c_char_p, P(vp)],
     "blest_bvss_destroy": [vp],
+    "blest_bvss_build_device": [vp, i32, P(vp)],
     "blest_bvss_edge_check": [vp, P(u64)],
     "blest_graph_create": [P(BvssView), P(CsrView), P(vp)],
+    "blest_graph_create_from_csc": [vp, vp, i32, P(vp)],
     "blest_graph_destroy": [vp],
     "blest_graph_info_get": [vp, P(GraphInfo)],
     "blest_graph_set_stream": [vp, vp],

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../host/errors.hpp"
+#include "../host/objects.hpp"
 #include "blest.h"
 #include "common.cuh"
 #include "runtime.hpp"
@@ -50,6 +51,8 @@ T* upload(blest_graph* g, const T* src, size_t count) {
     if (count) BLEST_CUDA(cudaMemcpy(d, src, count * sizeof(T), cudaMemcpyHostToDevice));
     return d;
 }
+
+void validate_csr(const blest_csr_view* c);
 
 // Structural checks the kernels rely on for memory safety (every index
 // they dereference is in range), done once at upload.
@@ -100,6 +103,12 @@ void validate_views(const blest_bvss_view* v, const blest_csr_view* c) {
     if (err & 8) bad("mask bit for a column >= n");
     if (!c) bad("the pull CSR is required (pass the transpose; for a symmetric graph, the CSC itself)");
     if (c->n != v->n) bad("CSR vertex count differs from the BVSS");
+    validate_csr(c);
+}
+
+void validate_csr(const blest_csr_view* c) {
+    auto bad = [](const std::string& m) { throw Error(BLEST_ERR_INVALID_ARG, "invalid graph: " + m); };
+    int err = 0;
     if (!c->row_ptrs || (c->nnz && !c->col_ids)) bad("null CSR array");
     if (c->row_ptrs[0] != 0 || c->row_ptrs[c->n] != c->nnz) bad("CSR row_ptrs ends");
 #pragma omp parallel for reduction(| : err) schedule(static, 4096)
@@ -327,6 +336,62 @@ int blest_init(int device) {
     });
 }
 
+}  // extern "C"
+
+namespace {
+
+// The pull side of a resident graph: CSR lists ordered by descending
+// neighbour degree, the has-in-neighbour bitmap and the long-list pieces;
+// then the graph's stream and default workspace.
+void graph_attach_csr(blest_graph* g, const blest_csr_view* csr) {
+    blest::dev::DevGraph& d = g->d;
+    d.nnz = csr->nnz;
+    d.degree_total = csr->nnz;
+    d.csr_ptrs = blest::upload(g, csr->row_ptrs, (size_t)csr->n + 1);
+    {
+        // Pull order: each vertex's in-neighbours by descending degree
+        // (ties by id). High-degree vertices join the frontier first in
+        // skewed graphs, so the bottom-up scan, which stops at the first
+        // frontier neighbour, stops sooner. Levels do not depend on the
+        // order; only which valid parent is recorded does.
+        std::vector<uint32_t> ids(csr->col_ids, csr->col_ids + csr->nnz);
+        const uint32_t* rp = csr->row_ptrs;
+#pragma omp parallel for schedule(dynamic, 1024)
+        for (int64_t u = 0; u < (int64_t)csr->n; ++u) {
+            std::stable_sort(ids.begin() + rp[u], ids.begin() + rp[u + 1], [rp](uint32_t x, uint32_t y) {
+                return rp[x + 1] - rp[x] > rp[y + 1] - rp[y];
+            });
+        }
+        d.csr_ids = blest::upload(g, ids.data(), ids.size());
+    }
+    {
+        std::vector<uint32_t> hasIn(((size_t)csr->n + 31) / 32 + 4, 0u);
+        for (uint32_t u = 0; u < csr->n; ++u)
+            if (csr->row_ptrs[u + 1] > csr->row_ptrs[u]) hasIn[u >> 5] |= 1u << (u & 31);
+        d.has_in = blest::upload(g, hasIn.data(), hasIn.size());
+    }
+    {
+        std::vector<uint4> chunks;
+        const uint32_t* rp = csr->row_ptrs;
+        for (uint32_t u = 0; u < csr->n; ++u)
+            if (rp[u + 1] - rp[u] > blest::dev::kPullChunk)
+                for (uint32_t e = rp[u]; e < rp[u + 1]; e += blest::dev::kPullChunk)
+                    chunks.push_back(make_uint4(u, e, std::min(e + blest::dev::kPullChunk, rp[u + 1]), 0u));
+        d.no_pull_chunks = (uint32_t)chunks.size();
+        d.pull_chunks = blest::upload(g, chunks.data(), chunks.size());
+    }
+    g->undirected_edges = csr->nnz / 2;
+    BLEST_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+    g->owns_stream = true;
+    g->default_ws = new blest_workspace;
+    g->default_ws->g = g;
+    blest::workspace_alloc(g, g->default_ws->w);
+}
+
+}  // namespace
+
+extern "C" {
+
 int blest_graph_create(const blest_bvss_view* bvss, const blest_csr_view* csr, blest_graph** out) {
     blest_graph* g = nullptr;
     const int rc = guarded([&] {
@@ -345,53 +410,53 @@ int blest_graph_create(const blest_bvss_view* bvss, const blest_csr_view* csr, b
         d.no_real = R;
         d.no_virtual = V;
         d.no_slices = bvss->no_slices;
-        d.nnz = csr->nnz;
-        d.degree_total = csr->nnz;
         d.slice_set_ptrs = blest::upload(g, bvss->slice_set_ptrs, (size_t)V + 1);
         d.virtual_to_real = blest::upload(g, bvss->virtual_to_real, V);
         d.real_ptrs = blest::upload(g, bvss->real_ptrs, (size_t)R + 1);
         d.row4 = (const uint4*)blest::upload(g, bvss->row_ids, bvss->no_slices);
         d.masks = blest::upload(g, bvss->masks, bvss->no_slices / 4);
         d.rset_tile = blest::upload(g, rsetTile.data(), rsetTile.size());
-        d.csr_ptrs = blest::upload(g, csr->row_ptrs, (size_t)csr->n + 1);
-        {
-            // Pull order: each vertex's in-neighbours by descending degree
-            // (ties by id). High-degree vertices join the frontier first in
-            // skewed graphs, so the bottom-up scan, which stops at the first
-            // frontier neighbour, stops sooner. Levels do not depend on the
-            // order; only which valid parent is recorded does.
-            std::vector<uint32_t> ids(csr->col_ids, csr->col_ids + csr->nnz);
-            const uint32_t* rp = csr->row_ptrs;
-#pragma omp parallel for schedule(dynamic, 1024)
-            for (int64_t u = 0; u < (int64_t)csr->n; ++u) {
-                std::stable_sort(ids.begin() + rp[u], ids.begin() + rp[u + 1], [rp](uint32_t x, uint32_t y) {
-                    return rp[x + 1] - rp[x] > rp[y + 1] - rp[y];
-                });
-            }
-            d.csr_ids = blest::upload(g, ids.data(), ids.size());
-        }
-        {
-            std::vector<uint32_t> hasIn(((size_t)csr->n + 31) / 32 + 4, 0u);
-            for (uint32_t u = 0; u < csr->n; ++u)
-                if (csr->row_ptrs[u + 1] > csr->row_ptrs[u]) hasIn[u >> 5] |= 1u << (u & 31);
-            d.has_in = blest::upload(g, hasIn.data(), hasIn.size());
-        }
-        {
-            std::vector<uint4> chunks;
-            const uint32_t* rp = csr->row_ptrs;
-            for (uint32_t u = 0; u < csr->n; ++u)
-                if (rp[u + 1] - rp[u] > blest::dev::kPullChunk)
-                    for (uint32_t e = rp[u]; e < rp[u + 1]; e += blest::dev::kPullChunk)
-                        chunks.push_back(make_uint4(u, e, std::min(e + blest::dev::kPullChunk, rp[u + 1]), 0u));
-            d.no_pull_chunks = (uint32_t)chunks.size();
-            d.pull_chunks = blest::upload(g, chunks.data(), chunks.size());
-        }
-        g->undirected_edges = csr->nnz / 2;
-        BLEST_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
-        g->owns_stream = true;
-        g->default_ws = new blest_workspace;
-        g->default_ws->g = g;
-        blest::workspace_alloc(g, g->default_ws->w);
+        graph_attach_csr(g, csr);
+        *out = g;
+    });
+    if (rc != BLEST_OK && g) blest_graph_destroy(g);
+    return rc;
+}
+
+int blest_graph_create_from_csc(const blest_csc* csc, const blest_csc* csr, int full_padding, blest_graph** out) {
+    blest_graph* g = nullptr;
+    const int rc = guarded([&] {
+        blest::require(csc && out, "null argument");
+        ensure_device();
+        const blest::Csc& c = csc->g;
+        const blest::Csc& t = csr ? csr->g : c;
+        if (!csr && !blest::csc_check_symmetry(c))
+            throw blest::Error(BLEST_ERR_INVALID_ARG, "a directed graph needs its transpose as the pull CSR");
+        if (t.n != c.n) throw blest::Error(BLEST_ERR_INVALID_ARG, "CSR vertex count differs from the CSC");
+        const blest_csr_view cv{t.n, t.nnz, t.col_ptrs.data(), t.rows.data()};
+        blest::validate_csr(&cv);
+        g = new blest_graph;
+        g->device = blest::g_device;
+        g->sm_count = blest::device_sm_count(g->device);
+        blest::DeviceBvss b;
+        blest::bvss_build_device(c, full_padding < 0 ? !c.is_social : full_padding != 0, nullptr, b);
+        for (void* p : {(void*)b.slice_set_ptrs, (void*)b.virtual_to_real, (void*)b.real_ptrs, (void*)b.row_ids,
+                        (void*)b.masks, (void*)b.rset_tile})
+            g->allocations.push_back(p);
+        g->graph_bytes += 8ull * (b.no_virtual + 1ull) + 4ull * b.no_virtual + 8ull * (b.no_real + 1ull) +
+                          5ull * b.no_slices;
+        blest::dev::DevGraph& d = g->d;
+        d.n = b.n;
+        d.no_real = b.no_real;
+        d.no_virtual = b.no_virtual;
+        d.no_slices = b.no_slices;
+        d.slice_set_ptrs = b.slice_set_ptrs;
+        d.virtual_to_real = b.virtual_to_real;
+        d.real_ptrs = b.real_ptrs;
+        d.row4 = (const uint4*)b.row_ids;
+        d.masks = b.masks;
+        d.rset_tile = b.rset_tile;
+        graph_attach_csr(g, &cv);
         *out = g;
     });
     if (rc != BLEST_OK && g) blest_graph_destroy(g);

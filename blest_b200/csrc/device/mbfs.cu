@@ -15,9 +15,15 @@
 //    atomicOr), or pull over the degree-ordered CSR (next[v] = OR of the
 //    in-neighbours' frontier words, stopping once every bit v still needs
 //    is covered);
-//  - sweep: new = next & ~visited; visited |= new; frontier = new; levels
-//    of the new (source, vertex) pairs written row by row (coalesced over
-//    32 consecutive vertices); rsets with new bits queued for a push.
+//  - sweep: new = next & ~visited; visited |= new; the new bits are level
+//    L's frontier, kept in history slot L % hist_slots; rsets with new bits
+//    queued for a push.
+// Levels are written once per (source, vertex), after the group's last
+// level, by one pass that reads the vertex's history slots and writes
+// every source row of 32 consecutive vertices at a time (full 128-byte
+// rows, no "unreached" pre-fill and no partial-sector writes per level).
+// When a group has more levels than slots, the oldest slots are written
+// out first (their sectors then take two partial writes).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -50,8 +56,12 @@ struct MbfsPart {
 struct MbfsArgs {
     DevGraph g;
     uint32_t* visited;   // n * WORDS
-    uint32_t* frontier;  // n * WORDS
     uint32_t* next;      // n * WORDS
+    // Frontier history: level L's new bits in slot L % hist_slots (n *
+    // WORDS words each; hist_slots a power of two, 2..64).
+    uint32_t* hist;
+    uint32_t hist_slots;
+    uint32_t* part_last;  // per part: last level whose slot it wrote in this group
     uint32_t* q_rset;    // 2 slots x qreg
     uint32_t* q_off;
     uint32_t qreg;
@@ -214,8 +224,8 @@ __device__ __forceinline__ void store_bits(uint32_t* a, uint32_t v, const Bits<W
 // to `need`; four neighbours' loads in flight at a time; stops once acc
 // covers need.
 template <int WORDS>
-__device__ __forceinline__ void scan_in_list(const MbfsArgs& a, uint32_t q, uint32_t qe, const uint32_t (&need)[WORDS],
-                                             uint32_t (&acc)[WORDS]) {
+__device__ __forceinline__ void scan_in_list(const MbfsArgs& a, const uint32_t* frontier, uint32_t q, uint32_t qe,
+                                             const uint32_t (&need)[WORDS], uint32_t (&acc)[WORDS]) {
     for (; q < qe; q += 4) {
         uint32_t u[4];
 #pragma unroll
@@ -224,7 +234,7 @@ __device__ __forceinline__ void scan_in_list(const MbfsArgs& a, uint32_t q, uint
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             if (u[j] != 0xFFFFFFFFu) {
-                f[j] = load_bits<WORDS>(a.frontier, u[j]);
+                f[j] = load_bits<WORDS>(frontier, u[j]);
             } else {
 #pragma unroll
                 for (int w = 0; w < WORDS; ++w) f[j].w[w] = 0u;
@@ -241,6 +251,65 @@ __device__ __forceinline__ void scan_in_list(const MbfsArgs& a, uint32_t q, uint
 }
 
 template <int WORDS>
+__device__ __forceinline__ uint32_t* hist_slot(const MbfsArgs& a, uint32_t level) {
+    return a.hist + (size_t)(level & (a.hist_slots - 1)) * a.g.n * WORDS;
+}
+
+// Levels [lo, min(hi, part_last[p])] of the group starting at source s0
+// into the output rows. A lane holds one vertex; one source word at a
+// time, it keeps the level offsets bit-sliced (bit j of plane j = bit j of
+// level - lo) and `found`, the sources of the word that reached the vertex
+// in those levels (a word's history loads after the first come from L2);
+// then each source row of the 32 vertices is one 128-byte store. final:
+// sources that never reached the vertex get 0xFFFFFFFF, sources that
+// reached it before lo (already written) are skipped; otherwise only found
+// ones are written.
+template <int WORDS>
+__device__ __forceinline__ void write_levels(const MbfsArgs& a, uint32_t warp, uint32_t nwarps, uint32_t s0,
+                                             uint32_t lo, uint32_t hi, bool final) {
+    const uint32_t lane = threadIdx.x & 31;
+    auto has_rows = [&](uint32_t, const MbfsPart& P) { return group_rows(P, s0, a.group_width) > 0; };
+    for_each_part_word(a, warp, nwarps, has_rows, [&](uint32_t p, const MbfsPart& P, uint32_t wi) {
+        const uint32_t v = wi * 32 + lane;
+        const uint32_t lv = v - P.off;
+        const bool in = lv < P.n;
+        const uint32_t rows = group_rows(P, s0, a.group_width);
+        const uint32_t top = min(hi, __ldcg(&a.part_last[p]));
+#pragma unroll
+        for (int w = 0; w < WORDS; ++w) {
+            const uint32_t rw = rows > 32u * w ? min(32u, rows - 32u * w) : 0u;
+            if (rw == 0) break;
+            uint32_t plane[6] = {0u, 0u, 0u, 0u, 0u, 0u}, found = 0u, vis = 0u;
+            if (in) {
+                for (uint32_t L = lo; L <= top && L != 0xFFFFFFFFu; ++L) {
+                    const uint32_t f = __ldcg(hist_slot<WORDS>(a, L) + (size_t)v * WORDS + w);
+                    const uint32_t rel = L - lo;
+                    found |= f;
+#pragma unroll
+                    for (int j = 0; j < 6; ++j)
+                        if ((rel >> j) & 1u) plane[j] |= f;
+                }
+                if (final) vis = __ldcg(a.visited + (size_t)v * WORDS + w);
+            }
+            for (uint32_t bit = 0; bit < rw; ++bit) {
+                uint32_t lvl;
+                if ((found >> bit) & 1u) {
+                    uint32_t rel = 0;
+#pragma unroll
+                    for (int j = 0; j < 6; ++j) rel |= ((plane[j] >> bit) & 1u) << j;
+                    lvl = lo + rel;
+                } else if (final && !((vis >> bit) & 1u)) {
+                    lvl = kUnreached;
+                } else {
+                    continue;
+                }
+                if (in) P.levels[(uint64_t)(s0 + 32u * w + bit) * P.n + lv] = lvl;
+            }
+        }
+    });
+}
+
+template <int WORDS>
 __global__ void __launch_bounds__(512, 2) mbfs_persistent_kernel(MbfsArgs a) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -249,24 +318,19 @@ __global__ void __launch_bounds__(512, 2) mbfs_persistent_kernel(MbfsArgs a) {
     const DevGraph& g = a.g;
     RunCounters* c = a.ctr;
     const uint32_t n = g.n;
-    const uint32_t Wn = (n + 31) / 32;
     auto barrier = [&]() -> bool { return grid_barrier(c); };
 
     for (uint32_t grp = 0; grp < a.groups; ++grp) {
         const uint32_t s0 = grp * a.group_width;
-        // ---- group init: state cleared, output rows of the group unreached
+        // ---- group init: visited, next and the level-0 history slot
+        // cleared (the output rows are written once, after the last level)
         for (uint32_t i = tid; i < n * WORDS; i += nth) {
             a.visited[i] = 0u;
-            a.frontier[i] = 0u;
+            a.hist[i] = 0u;  // slot 0
             a.next[i] = 0u;
         }
-        for (uint32_t wi = warp; wi < Wn; wi += nwarps) {
-            const MbfsPart P = load_part(a, part_of_word(a, wi));
-            const uint32_t rows = group_rows(P, s0, a.group_width);
-            const uint32_t lv = wi * 32 + lane - P.off;
-            if (lv < P.n)
-                for (uint32_t b = 0; b < rows; ++b) P.levels[(uint64_t)(s0 + b) * P.n + lv] = kUnreached;
-        }
+        for (uint32_t p = tid; p < a.nparts; p += nth) a.part_last[p] = 0u;
+        uint32_t base = 0;  // first level not yet written to the output
         if (tid == 0) {
             c->aux[0] = c->aux[1] = 0;  // push queue counters (2 slots)
             c->aux[4] = c->aux[5] = 0;  // new-frontier vertex counts (2 slots)
@@ -291,8 +355,7 @@ __global__ void __launch_bounds__(512, 2) mbfs_persistent_kernel(MbfsArgs a) {
                         } else {
                             const uint32_t v = P.off + src;
                             atomicOr(&a.visited[v * WORDS + (b >> 5)], 1u << (b & 31));
-                            atomicOr(&a.frontier[v * WORDS + (b >> 5)], 1u << (b & 31));
-                            P.levels[(uint64_t)(s0 + b) * P.n + src] = 0u;
+                            atomicOr(&a.hist[v * WORDS + (b >> 5)], 1u << (b & 31));
                             atomicAdd(&a.part_nf[p], 1u);  // level-0 slot
                             ++seeded;
                             r = v >> 3;
@@ -349,6 +412,14 @@ __global__ void __launch_bounds__(512, 2) mbfs_persistent_kernel(MbfsArgs a) {
                 set_error(c, BLEST_ERR_LEVEL_CAP);
                 return;
             }
+            // slot level % hist_slots still holds unwritten level `base`:
+            // write levels [base, level) out first (the sweep that reuses
+            // the slot comes after the next barrier)
+            if (level - base == a.hist_slots) {
+                write_levels<WORDS>(a, warp, nwarps, s0, base, level - 1, false);
+                base = level;
+            }
+
             if (tid == 0) {
                 c->aux[slot ^ 1] = 0;      // queue slot the coming sweep fills
                 c->aux[4 + (slot ^ 1)] = 0;
@@ -384,7 +455,7 @@ __global__ void __launch_bounds__(512, 2) mbfs_persistent_kernel(MbfsArgs a) {
                     any |= need[w] != 0;
                 }
                 if (!any) return;
-                scan_in_list<WORDS>(a, pb, pe, need, acc);
+                scan_in_list<WORDS>(a, hist_slot<WORDS>(a, level - 1), pb, pe, need, acc);
                 bool got = false;
                 Bits<WORDS> out;
 #pragma unroll
@@ -410,7 +481,7 @@ __global__ void __launch_bounds__(512, 2) mbfs_persistent_kernel(MbfsArgs a) {
                         any |= need[w] != 0;
                     }
                     if (!any) continue;
-                    scan_in_list<WORDS>(a, piece.y, piece.z, need, acc);
+                    scan_in_list<WORDS>(a, hist_slot<WORDS>(a, level - 1), piece.y, piece.z, need, acc);
 #pragma unroll
                     for (int w = 0; w < WORDS; ++w)
                         if (acc[w]) atomicOr(&a.next[v * WORDS + w], acc[w]);
@@ -478,7 +549,7 @@ __global__ void __launch_bounds__(512, 2) mbfs_persistent_kernel(MbfsArgs a) {
                         Bits<WORDS> fc;
 #pragma unroll
                         for (int w = 0; w < WORDS; ++w) fc.w[w] = 0u;
-                        if (lane < 8 && r * 8 + lane < n) fc = load_bits<WORDS>(a.frontier, r * 8 + lane);
+                        if (lane < 8 && r * 8 + lane < n) fc = load_bits<WORDS>(hist_slot<WORDS>(a, level - 1), r * 8 + lane);
                         uint4 rows = make_uint4(0, 0, 0, 0);
                         uint32_t mask = 0;
                         if (tile < t1) {
@@ -539,12 +610,10 @@ __global__ void __launch_bounds__(512, 2) mbfs_persistent_kernel(MbfsArgs a) {
                         nv.w[w] = vis.w[w] | nw.w[w];
                         any |= nw.w[w] != 0;
                     }
-                    const Bits<WORDS> fr = load_bits<WORDS>(a.frontier, v);
-                    bool frAny = false;
-#pragma unroll
-                    for (int w = 0; w < WORDS; ++w) frAny |= fr.w[w] != 0;
                     if (any) store_bits<WORDS>(a.visited, v, nv);
-                    if (any || frAny) store_bits<WORDS>(a.frontier, v, nw);
+                    // every word of an active graph: the slot held an
+                    // older level
+                    store_bits<WORDS>(hist_slot<WORDS>(a, level), v, nw);
                     bool nxAny = false;
 #pragma unroll
                     for (int w = 0; w < WORDS; ++w) nxAny |= nx.w[w] != 0;
@@ -558,22 +627,11 @@ __global__ void __launch_bounds__(512, 2) mbfs_persistent_kernel(MbfsArgs a) {
 #pragma unroll
                     for (int w = 0; w < WORDS; ++w) nw.w[w] = 0u;
                 }
+                if (lane == 0 && wi * 32 == P.off) a.part_last[p] = level;  // the graph's slot for `level` is valid
                 const uint32_t anyMask = __ballot_sync(0xFFFFFFFFu, any);
                 if (!anyMask) return;
                 cnt += any ? 1u : 0u;
                 if (lane == 0) atomicAdd(&nfn[p], (uint32_t)__popc(anyMask));
-                // levels of the new (source, vertex) pairs, one source row at
-                // a time (new bits only arise in real vertices of the graph)
-                const uint32_t lv = v - P.off;
-#pragma unroll
-                for (int w = 0; w < WORDS; ++w) {
-                    uint32_t rowsAny = __reduce_or_sync(0xFFFFFFFFu, nw.w[w]);
-                    while (rowsAny) {
-                        const uint32_t b = __ffs(rowsAny) - 1;
-                        rowsAny &= rowsAny - 1;
-                        if ((nw.w[w] >> b) & 1u) P.levels[(uint64_t)(s0 + 32 * w + b) * P.n + lv] = level;
-                    }
-                }
                 // queue rsets with new bits (lanes 8j..8j+7 share rset)
                 const uint32_t grpBits = (anyMask >> (lane & ~7u)) & 0xFFu;
                 uint64_t mine = 0;
@@ -606,6 +664,9 @@ __global__ void __launch_bounds__(512, 2) mbfs_persistent_kernel(MbfsArgs a) {
             if (tid == 0) c->levels = max(c->levels, level);
             if (!barrier()) return;
         }
+        // ---- every output row of the group, once
+        write_levels<WORDS>(a, warp, nwarps, s0, base, 0xFFFFFFFEu, true);
+        if (!barrier()) return;
     }
 }
 
@@ -614,12 +675,14 @@ __global__ void __launch_bounds__(512, 2) mbfs_persistent_kernel(MbfsArgs a) {
 namespace {
 
 struct MbfsScratch {
-    uint32_t* state = nullptr;  // visited | frontier | next
+    uint32_t* state = nullptr;  // visited | next | frontier history slots
     uint32_t* levels = nullptr; // staging for host output
     uint32_t* sources = nullptr;
     uint32_t* queue = nullptr;  // rset queue: 2 slots of entries + 2 slots of offsets
     uint32_t* part_nf = nullptr;  // per-graph frontier counts, 2 slots
-    size_t state_words = 0, levels_words = 0, sources_cap = 0, queue_words = 0, part_nf_cap = 0;
+    uint32_t* part_last = nullptr;  // per-graph last level with a valid history slot
+    size_t state_words = 0, levels_words = 0, sources_cap = 0, queue_words = 0, part_nf_cap = 0,
+           part_last_cap = 0;
 };
 
 // Entries one queue slot needs: a sweep queues each rset at most once; the
@@ -649,12 +712,16 @@ template <int WORDS>
 void prepare_words(const blest_graph* g, blest::Workspace& w, MbfsScratch& sc, const blest_mbfs_params& p,
                    uint64_t seeds, uint32_t nparts, MbfsLaunch& L) {
     const uint32_t n = g->d.n;
-    ensure(sc.state, sc.state_words, 3ull * n * WORDS);
+    const uint32_t slots = mbfs_history_slots(n, WORDS);
+    ensure(sc.state, sc.state_words, mbfs_state_words(n, WORDS));
     dev::MbfsArgs& a = L.a;
     a.g = g->d;
     a.visited = sc.state;
-    a.frontier = sc.state + (size_t)n * WORDS;
-    a.next = sc.state + 2ull * n * WORDS;
+    a.next = sc.state + (size_t)n * WORDS;
+    a.hist = sc.state + 2ull * n * WORDS;
+    a.hist_slots = slots;
+    ensure(sc.part_last, sc.part_last_cap, nparts);
+    a.part_last = sc.part_last;
     a.qreg = mbfs_queue_slot(g->d.no_real, seeds);
     ensure(sc.queue, sc.queue_words, 4ull * a.qreg);
     a.q_rset = sc.queue;
@@ -699,13 +766,25 @@ void issue_mbfs(const MbfsLaunch& L, cudaStream_t s) {
 
 }  // namespace
 
+uint32_t mbfs_history_slots(uint32_t n, uint32_t words) {
+    const uint64_t slot = 4ull * n * words;
+    uint32_t k = 64;  // a power of two: the kernel takes level % slots as a mask
+    while (k > 2 && (uint64_t)k * slot > kMbfsHistoryBytes) k >>= 1;
+    return k;
+}
+
+uint64_t mbfs_state_words(uint32_t n, uint32_t words) {
+    return (2ull + mbfs_history_slots(n, words)) * n * words;
+}
+
 void mbfs_reserve(Workspace& w, uint32_t n, uint32_t words) {
     if (!w.mbfs) w.mbfs = new MbfsScratch;
     MbfsScratch& sc = *(MbfsScratch*)w.mbfs;
-    ensure(sc.state, sc.state_words, 3ull * n * words);
+    ensure(sc.state, sc.state_words, mbfs_state_words(n, words));
     ensure(sc.sources, sc.sources_cap, 128);
     ensure(sc.queue, sc.queue_words, 4ull * mbfs_queue_slot((n + 7) / 8, 32u * words));
     ensure(sc.part_nf, sc.part_nf_cap, 2);
+    ensure(sc.part_last, sc.part_last_cap, 1);
 }
 
 void mbfs_scratch_free(void* p) {
@@ -716,6 +795,7 @@ void mbfs_scratch_free(void* p) {
     cudaFree(sc->sources);
     cudaFree(sc->queue);
     cudaFree(sc->part_nf);
+    cudaFree(sc->part_last);
     delete sc;
 }
 

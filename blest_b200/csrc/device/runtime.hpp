@@ -12,6 +12,7 @@
 #include "blest.h"
 #include "common.cuh"
 #include "../host/common.hpp"
+#include "../host/csc.hpp"
 
 namespace blest {
 
@@ -113,9 +114,32 @@ void launch_bfs(const blest_graph* g, Workspace& w, uint32_t src, uint32_t* leve
 void launch_cc(const blest_graph* g, Workspace& w, uint32_t* labels, cudaStream_t s);
 
 int device_sm_count(int device);
+
+// A BVSS built on the device (bvss_build.cu): the reference's arrays plus
+// the derived rset tile table, in device memory the caller owns.
+struct DeviceBvss {
+    uint32_t n = 0, no_real = 0, no_virtual = 0;
+    uint64_t no_slices = 0, no_padded = 0;
+    double update_divergence = 0;
+    bool full_padding = false;
+    uint64_t* slice_set_ptrs = nullptr;
+    uint32_t* virtual_to_real = nullptr;
+    uint32_t* real_ptrs = nullptr;
+    uint32_t* row_ids = nullptr;
+    uint32_t* masks = nullptr;
+    uint32_t* rset_tile = nullptr;
+};
+void bvss_build_device(const Csc& g, bool full_padding, cudaStream_t s, DeviceBvss& out);
+void device_bvss_free(DeviceBvss& b);
 void mbfs_scratch_free(void* p);
 // Allocate the multi-source BFS state of `words` 32-bit words per vertex now.
 void mbfs_reserve(Workspace& w, uint32_t n, uint32_t words);
+// Multi-source BFS state: visited, next and the frontier history: the
+// largest power of two of slots (2..64, n * words words each) that fits
+// kMbfsHistoryBytes.
+constexpr uint64_t kMbfsHistoryBytes = 1ull << 30;
+uint32_t mbfs_history_slots(uint32_t n, uint32_t words);
+uint64_t mbfs_state_words(uint32_t n, uint32_t words);
 // Cooperative grid: occupancy maximum, optionally capped by the workspace.
 inline int cooperative_grid(int max_blocks_per_sm, int sm_count, uint32_t cap) {
     const int full = max_blocks_per_sm * sm_count;

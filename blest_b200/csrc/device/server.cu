@@ -109,7 +109,7 @@ double now(const blest_server* s) { return std::chrono::duration<double>(Clock::
 uint64_t job_bytes(const GraphEntry& ge, int kind, uint32_t k) {
     if (kind == BLEST_QUERY_CC || k <= 1) return 0;
     const uint64_t words = k <= 32 ? 1 : (k <= 64 ? 2 : 4);
-    return 3ull * ge.n * 4 * words + 4ull * k * ge.n;  // MBFS state + staged levels
+    return 4ull * mbfs_state_words(ge.n, (uint32_t)words) + 4ull * k * ge.n;  // MBFS state + staged levels
 }
 
 void finish(blest_server* s, Job& job, int status, const std::string& err, double start) {

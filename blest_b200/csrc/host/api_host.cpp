@@ -6,18 +6,13 @@
 #include <string>
 
 #include "blest.h"
+#include "objects.hpp"
 #include "bvss.hpp"
 #include "csc.hpp"
 #include "errors.hpp"
 #include "generators.hpp"
 #include "reorder.hpp"
 
-struct blest_csc {
-    blest::Csc g;
-};
-struct blest_bvss {
-    blest::Bvss b;
-};
 
 using blest::guarded;
 
@@ -146,7 +141,8 @@ int blest_csc_reorder(blest_csc* g, const blest_order_params* p, uint32_t* inver
             case BLEST_ORDER_RANDOM: inv = blest::order_random(g->g, p->seed); break;
             case BLEST_ORDER_DEGREE: inv = blest::order_degree(g->g, true); break;
             case BLEST_ORDER_GORDER:
-                inv = blest::order_gorder(g->g, p->window ? p->window : blest::kSliceSize);
+                // CSC::gorder(sliceSize): the greedy's window is the slice size
+                inv = blest::order_gorder(g->g, blest::kSliceSize);
                 break;
             default: throw blest::Error(BLEST_ERR_INVALID_ARG, "unknown ordering mode");
         }

@@ -355,9 +355,3 @@ std::vector<uint32_t> order_rcm(const Csc& g0, uint32_t rand_seed) {
 }
 
 }  // namespace blest
-
-namespace blest {
-std::vector<uint32_t> order_gorder(const Csc&, uint32_t) {
-    throw Error(BLEST_ERR_UNSUPPORTED, "Gorder ordering is not built yet");
-}
-}  // namespace blest

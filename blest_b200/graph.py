@@ -200,6 +200,16 @@ class Bvss:
         return cls(h)
 
     @classmethod
+    def build_device(cls, csc: Csc, full_padding: bool | None = None) -> "Bvss":
+        """The same BVSS built by GPU kernels (blest_bvss_build_device)."""
+        if not _initialised:
+            init(0)
+        h = C.c_void_p()
+        fp = -1 if full_padding is None else int(full_padding)
+        L.call("blest_bvss_build_device", csc._h, fp, C.byref(h))
+        return cls(h)
+
+    @classmethod
     def load_bin(cls, path: str) -> "Bvss":
         h = C.c_void_p()
         L.call("blest_bvss_load_bin", str(path).encode(), C.byref(h))
@@ -311,6 +321,21 @@ class Graph:
         L.call("blest_graph_create", C.byref(v), C.byref(cs), C.byref(h))
         self._h = h
         self.n = v.n
+
+    @classmethod
+    def from_csc(cls, csc: Csc, csr: Csc | None = None, full_padding: bool | None = None) -> "Graph":
+        """Resident graph whose BVSS is built on the device from `csc`
+        (blest_graph_create_from_csc); `csr` = pull CSR, None for a
+        symmetric CSC."""
+        if not _initialised:
+            init(0)
+        g = cls.__new__(cls)
+        h = C.c_void_p()
+        fp = -1 if full_padding is None else int(full_padding)
+        L.call("blest_graph_create_from_csc", csc._h, csr._h if csr is not None else None, fp, C.byref(h))
+        g._h = h
+        g.n = csc.n
+        return g
 
     def close(self) -> None:
         h = getattr(self, "_h", None)

@@ -174,6 +174,10 @@ int blest_bvss_view_get(const blest_bvss* b, blest_bvss_view* out);
 int blest_bvss_save_bin(const blest_bvss* b, const char* path);
 int blest_bvss_load_bin(const char* path, blest_bvss** out);
 int blest_bvss_destroy(blest_bvss* b);
+/* blest_bvss_build on the GPU (current device): kernels build the arrays in
+ * device memory, which are then copied into the returned host BVSS; the
+ * result is identical to blest_bvss_build's (update divergence included). */
+int blest_bvss_build_device(const blest_csc* g, int full_padding, blest_bvss** out);
 /* popcount of all masks (the reference's "Check" line, BVSS.cuh:508-538). */
 int blest_bvss_edge_check(const blest_bvss* b, uint64_t* edges);
 
@@ -210,6 +214,13 @@ typedef struct blest_graph_info {
  * graph is symmetric (the BVSS's own CSC is then used for pull: the
  * caller passes it as `csr` anyway, or BFS runs push-only). */
 int blest_graph_create(const blest_bvss_view* bvss, const blest_csr_view* csr, blest_graph** out);
+/* The same resident graph built from a CSC, with the BVSS constructed on
+ * the device (BVSS::constructFromCSCMatrix, BVSS.cuh:185-418, done by
+ * GPU kernels instead of the host merge; the arrays are those
+ * blest_bvss_build makes, byte for byte). `csr` is the pull CSR (the
+ * CSC's transpose), or NULL for a symmetric CSC (then the CSC itself).
+ * full_padding < 0: as the reference, !is_social. */
+int blest_graph_create_from_csc(const blest_csc* csc, const blest_csc* csr, int full_padding, blest_graph** out);
 int blest_graph_destroy(blest_graph* g);
 int blest_graph_info_get(const blest_graph* g, blest_graph_info* out);
 /* Stream used by calls that do not take a workspace. */

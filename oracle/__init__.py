@@ -267,7 +267,7 @@ class RefGraph:
     def reorder(self, mode: str, window: int = 65536, rand_seed: int = 1) -> np.ndarray:
         n, nnz, cp, rw = self.csc()
         inv = np.empty(n, dtype=np.uint32)
-        m = {"natural": 1, "jaccard": 2, "rcm": 3}[mode]
+        m = {"natural": 1, "jaccard": 2, "rcm": 3, "gorder": 4}[mode]
         _rcheck(rlib().ref_csc_reorder(self.h, m, window, rand_seed, _p32(inv)))
         return inv
 

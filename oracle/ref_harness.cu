@@ -119,7 +119,8 @@ int ref_csc_is_social(void* h, int* social) {
 }
 
 /* mode 1 = natural, 2 = jackardWithWindow(8, window), 3 = rcm() with the C
- * library rand() reseeded to `rand_seed` first (1 = never-seeded state).
+ * library rand() reseeded to `rand_seed` first (1 = never-seeded state),
+ * 4 = gorder(8) (the vendored Gorder greedy, CSC.cuh:950-966).
  * The permutation is applied to the CSC (as CSC::reorder does) and copied
  * to inv_out[n]. */
 int ref_csc_reorder(void* h, int mode, uint32_t window, uint32_t rand_seed, uint32_t* inv_out) {
@@ -136,6 +137,8 @@ int ref_csc_reorder(void* h, int mode, uint32_t window, uint32_t rand_seed, uint
         } else if (mode == 3) {
             srand(rand_seed);
             inv = c->rcm();
+        } else if (mode == 4) {
+            inv = c->gorder(8);
         } else {
             throw std::runtime_error("bad mode");
         }

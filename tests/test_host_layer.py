@@ -174,3 +174,20 @@ def test_rcm_matches_reference_on_parallel_levels(make):
     c = make()
     want = O.RefGraph.from_csc(c.n, c.col_ptrs, c.rows).reorder("rcm")
     np.testing.assert_array_equal(c.reorder("rcm"), want)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference harness not built")
+@pytest.mark.parametrize("make", [
+    lambda: Csc.rmat(12, 8, seed=3, permute_seed=2),
+    lambda: Csc.rmat(14, 16, seed=5, permute_seed=1),
+    lambda: Csc.grid(60, 40, 0.05, 0.01, seed=2),
+    lambda: Csc.er(2000, 1500, seed=7),  # isolated vertices
+    lambda: Csc.from_edges(300, *zip(*[(i, (i * 7 + 3) % 300) for i in range(300)])),  # directed
+], ids=["rmat12", "rmat14", "grid60x40", "er_isolated", "directed300"])
+def test_gorder_matches_reference(make):
+    """BLEST_ORDER_GORDER gives the permutation of the reference's
+    CSC::gorder(8) (the vendored Gorder greedy, run through the harness)."""
+    c = make()
+    want = O.RefGraph.from_csc(c.n, c.col_ptrs, c.rows).reorder("gorder")
+    got = c.reorder("gorder")
+    np.testing.assert_array_equal(np.asarray(got), want)
