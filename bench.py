@@ -791,7 +791,7 @@ def run_b200(args, rank, world):
     out = torch.empty(n, dtype=torch.int32, device="cuda")
     barrier = (lambda: dist.barrier()) if world > 1 else (lambda: None)
 
-    params = bfs_params("auto", args.slice_test)
+    params = bfs_params(args.direction, args.slice_test)
     tuned = None
     if args.autotune:
         from blest_b200.autotune import tune_bfs
@@ -923,7 +923,7 @@ def run_b200(args, rank, world):
         # per-level records of a few traced BFS runs (diagnostics, stderr)
         from blest_b200 import _lib as L
         import ctypes as C
-        tp = bfs_params("auto", args.slice_test, trace=True)
+        tp = bfs_params(args.direction, args.slice_test, trace=True)
         recs = (L.LevelTrace * 4096)()
         for s in sources[: args.trace_levels]:
             ws.bfs_async(int(s), out.data_ptr(), sptr, params=tp)
@@ -948,7 +948,8 @@ def run_b200(args, rank, world):
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generator; see config)",
         "config": bfs_config(args.workload, n, csc.nnz, len(sources), edges_per_step, info.no_slices, world),
         "impl_detail": {"bfs_params": tuned or f"defaults (alpha 14, beta 24, occupancy grid, "
-                                                 f"{args.slice_test} slice test)",
+                                                 f"{args.slice_test} slice test, direction {args.direction})",
+                        "device_tiles": int(info.device_tiles),
                         "graph_bytes_hbm": int(info.device_bytes_graph)},
         "value_reference_timing": {"value": round(value_wall, 3), "unit": "GTEPS",
                                    "note": "host wall time launch -> synchronise per BFS, the reference's "
@@ -1236,6 +1237,8 @@ def main():
     ap.add_argument("--cache", default="/tmp/blest_bench_cache")
     ap.add_argument("--ref-sources", type=int, default=8,
                     help="reference arm: sources per timed step (each call re-uploads the graph)")
+    ap.add_argument("--direction", choices=["auto", "push", "pull"], default="auto",
+                    help="BFS direction policy (push-only is the reference's eager kernel's schedule)")
     ap.add_argument("--slice-test", choices=["cuda_core", "mma"], default="cuda_core",
                     help="BFS slice test: CUDA-core byte AND, or the b1 mma.sync m8n8k128 AND+POPC")
     ap.add_argument("--no-cpu-baseline", action="store_true")

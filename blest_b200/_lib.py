@@ -75,7 +75,7 @@ class CsrView(C.Structure):
 class GraphInfo(C.Structure):
     _fields_ = [("n", u32), ("no_real_slice_sets", u32), ("no_virtual_slice_sets", u32), ("no_slices", u64),
                 ("nnz", u32), ("undirected_edges", u64), ("device_bytes_graph", u64),
-                ("device_bytes_workspace", u64), ("device", i32)]
+                ("device_bytes_workspace", u64), ("device", i32), ("device_tiles", u64)]
 
 
 class BfsParams(C.Structure):

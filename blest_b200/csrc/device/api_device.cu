@@ -340,6 +340,19 @@ int blest_init(int device) {
 
 namespace {
 
+// The kernels' tiles of a graph from its BVSS slices (device arrays, not
+// taken over): compacted into allocations the graph owns.
+void attach_tiles(blest_graph* g, const uint32_t* rows, const uint32_t* masks, const uint32_t* rset_tile) {
+    blest::CompactTiles t;
+    blest::compact_tiles_device(rows, masks, rset_tile, g->d.no_real, nullptr, t);
+    for (void* p : {(void*)t.row_ids, (void*)t.masks, (void*)t.rset_tile}) g->allocations.push_back(p);
+    g->graph_bytes += 20ull * t.tiles + 4ull * (g->d.no_real + 1ull);
+    g->d.no_slices = 4ull * t.tiles;
+    g->d.row4 = (const uint4*)t.row_ids;
+    g->d.masks = t.masks;
+    g->d.rset_tile = t.rset_tile;
+}
+
 // The pull side of a resident graph: CSR lists ordered by descending
 // neighbour degree, the has-in-neighbour bitmap and the long-list pieces;
 // then the graph's stream and default workspace.
@@ -401,21 +414,40 @@ int blest_graph_create(const blest_bvss_view* bvss, const blest_csr_view* csr, b
         g = new blest_graph;
         g->device = blest::g_device;
         g->sm_count = blest::device_sm_count(g->device);
-        const uint32_t R = bvss->no_real_slice_sets, V = bvss->no_virtual_slice_sets;
-        // Tile range of every rset (4 slices per tile).
+        const uint32_t R = bvss->no_real_slice_sets;
+        // Tile range of every rset in the BVSS (4 slices per tile).
         std::vector<uint32_t> rsetTile((size_t)R + 1);
         for (uint32_t r = 0; r <= R; ++r) rsetTile[r] = (uint32_t)(bvss->slice_set_ptrs[bvss->real_ptrs[r]] / 4);
-        blest::dev::DevGraph& d = g->d;
-        d.n = bvss->n;
-        d.no_real = R;
-        d.no_virtual = V;
-        d.no_slices = bvss->no_slices;
-        d.slice_set_ptrs = blest::upload(g, bvss->slice_set_ptrs, (size_t)V + 1);
-        d.virtual_to_real = blest::upload(g, bvss->virtual_to_real, V);
-        d.real_ptrs = blest::upload(g, bvss->real_ptrs, (size_t)R + 1);
-        d.row4 = (const uint4*)blest::upload(g, bvss->row_ids, bvss->no_slices);
-        d.masks = blest::upload(g, bvss->masks, bvss->no_slices / 4);
-        d.rset_tile = blest::upload(g, rsetTile.data(), rsetTile.size());
+        g->d.n = bvss->n;
+        g->d.no_real = R;
+        g->bvss_virtual = bvss->no_virtual_slice_sets;
+        g->bvss_slices = bvss->no_slices;
+        {
+            // staged BVSS slices, compacted into the kernels' tiles
+            blest::dev::DevGraph& d = g->d;
+            uint32_t *rows = nullptr, *masks = nullptr, *rt = nullptr;
+            auto release = [&] {
+                cudaFree(rows);
+                cudaFree(masks);
+                cudaFree(rt);
+            };
+            try {
+                BLEST_CUDA(cudaMalloc((void**)&rows, std::max<size_t>(4ull * bvss->no_slices, 16)));
+                BLEST_CUDA(cudaMalloc((void**)&masks, std::max<size_t>(bvss->no_slices, 4)));
+                BLEST_CUDA(cudaMalloc((void**)&rt, 4ull * (R + 1)));
+                if (bvss->no_slices) {
+                    BLEST_CUDA(cudaMemcpy(rows, bvss->row_ids, 4ull * bvss->no_slices, cudaMemcpyHostToDevice));
+                    BLEST_CUDA(cudaMemcpy(masks, bvss->masks, bvss->no_slices, cudaMemcpyHostToDevice));
+                }
+                BLEST_CUDA(cudaMemcpy(rt, rsetTile.data(), 4ull * (R + 1), cudaMemcpyHostToDevice));
+                attach_tiles(g, rows, masks, rt);
+            } catch (...) {
+                release();
+                throw;
+            }
+            release();
+            (void)d;
+        }
         graph_attach_csr(g, csr);
         *out = g;
     });
@@ -440,22 +472,17 @@ int blest_graph_create_from_csc(const blest_csc* csc, const blest_csc* csr, int 
         g->sm_count = blest::device_sm_count(g->device);
         blest::DeviceBvss b;
         blest::bvss_build_device(c, full_padding < 0 ? !c.is_social : full_padding != 0, nullptr, b);
-        for (void* p : {(void*)b.slice_set_ptrs, (void*)b.virtual_to_real, (void*)b.real_ptrs, (void*)b.row_ids,
-                        (void*)b.masks, (void*)b.rset_tile})
-            g->allocations.push_back(p);
-        g->graph_bytes += 8ull * (b.no_virtual + 1ull) + 4ull * b.no_virtual + 8ull * (b.no_real + 1ull) +
-                          5ull * b.no_slices;
-        blest::dev::DevGraph& d = g->d;
-        d.n = b.n;
-        d.no_real = b.no_real;
-        d.no_virtual = b.no_virtual;
-        d.no_slices = b.no_slices;
-        d.slice_set_ptrs = b.slice_set_ptrs;
-        d.virtual_to_real = b.virtual_to_real;
-        d.real_ptrs = b.real_ptrs;
-        d.row4 = (const uint4*)b.row_ids;
-        d.masks = b.masks;
-        d.rset_tile = b.rset_tile;
+        g->d.n = b.n;
+        g->d.no_real = b.no_real;
+        g->bvss_virtual = b.no_virtual;
+        g->bvss_slices = b.no_slices;
+        try {
+            attach_tiles(g, b.row_ids, b.masks, b.rset_tile);
+        } catch (...) {
+            blest::device_bvss_free(b);
+            throw;
+        }
+        blest::device_bvss_free(b);
         graph_attach_csr(g, &cv);
         *out = g;
     });
@@ -483,8 +510,9 @@ int blest_graph_info_get(const blest_graph* g, blest_graph_info* out) {
         blest::require(g && out, "null argument");
         out->n = g->d.n;
         out->no_real_slice_sets = g->d.no_real;
-        out->no_virtual_slice_sets = g->d.no_virtual;
-        out->no_slices = g->d.no_slices;
+        out->no_virtual_slice_sets = g->bvss_virtual;
+        out->no_slices = g->bvss_slices;
+        out->device_tiles = g->d.no_slices / 4;
         out->nnz = g->d.nnz;
         out->undirected_edges = g->undirected_edges;
         out->device_bytes_graph = g->graph_bytes;

@@ -1012,8 +1012,6 @@ extern "C" int blest_bfs_noalloc(const blest_device_graph_view* g, uint32_t sour
         a.g.nnz = g->nnz;
         a.g.no_slices = g->no_slices;
         a.g.degree_total = g->nnz;
-        a.g.slice_set_ptrs = g->slice_set_ptrs;
-        a.g.real_ptrs = g->real_ptrs;
         a.g.row4 = (const uint4*)g->row_ids;
         a.g.masks = g->masks;
         a.g.rset_tile = (const uint32_t*)(base + kNaRsetTile);

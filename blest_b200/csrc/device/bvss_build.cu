@@ -212,6 +212,78 @@ __global__ void bvss_divergence_kernel(const uint64_t* ssp, const uint32_t* row_
     }
 }
 
+// Tile compaction (the device copy the kernels read): per rset, the
+// slices with a non-zero mask, in their original order, 4 per tile, the
+// rset's last tile padded (row 0xFFFFFFFF, mask 0). Full padding (the
+// reference's layout for high-diameter graphs, BVSS.cuh:356-378) leaves
+// most slices empty; this copy drops them.
+__global__ void __launch_bounds__(256) compact_count_kernel(const uint32_t* masks, const uint32_t* rset_tile,
+                                                            uint32_t R, uint32_t* tiles) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t r = warp; r <= R; r += nwarps) {
+        if (r == R) {
+            if (lane == 0) tiles[R] = 0;
+            continue;
+        }
+        const uint32_t t0 = __ldg(&rset_tile[r]), t1 = __ldg(&rset_tile[r + 1]);
+        uint32_t c = 0;
+        for (uint32_t t = t0 + lane; t < t1; t += 32) {
+            const uint32_t m = __ldg(&masks[t]);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) c += ((m >> (8 * k)) & 0xFFu) != 0;
+        }
+        c = __reduce_add_sync(kFull, c);
+        if (lane == 0) tiles[r] = (c + 3) / 4;
+    }
+}
+
+__global__ void __launch_bounds__(256) compact_fill_kernel(const uint4* rows4, const uint32_t* masks,
+                                                           const uint32_t* rset_tile, const uint32_t* new_tile,
+                                                           uint32_t R, uint32_t* out_rows, uint8_t* out_mask_bytes) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t below = (1u << lane) - 1;
+    for (uint32_t r = warp; r < R; r += nwarps) {
+        const uint32_t t0 = __ldg(&rset_tile[r]), t1 = __ldg(&rset_tile[r + 1]);
+        uint64_t pos = 4ull * __ldg(&new_tile[r]);
+        for (uint32_t base = t0; base < t1; base += 32) {
+            const uint32_t t = base + lane;
+            uint32_t m = 0;
+            uint4 rw = make_uint4(0, 0, 0, 0);
+            if (t < t1) {
+                m = __ldg(&masks[t]);
+                rw = __ldg(&rows4[t]);
+            }
+            uint32_t c = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) c += ((m >> (8 * k)) & 0xFFu) != 0;
+            // exclusive prefix of the lanes' counts (each count <= 4)
+            uint32_t incl = c;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t o = __shfl_up_sync(kFull, incl, d);
+                if (lane >= (uint32_t)d) incl += o;
+            }
+            uint64_t q = pos + incl - c;
+            const uint32_t rk[4] = {rw.x, rw.y, rw.z, rw.w};
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const uint32_t mb = (m >> (8 * k)) & 0xFFu;
+                if (mb) {
+                    out_rows[q] = rk[k];
+                    out_mask_bytes[q] = (uint8_t)mb;
+                    ++q;
+                }
+            }
+            pos += __shfl_sync(kFull, incl, 31);
+            (void)below;
+        }
+    }
+}
+
 __global__ void rset_tile_kernel(const uint64_t* slice_off, uint32_t R, uint32_t* rset_tile) {
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r <= R; r += gridDim.x * blockDim.x)
         rset_tile[r] = (uint32_t)(slice_off[r] / 4);
@@ -322,6 +394,39 @@ void bvss_build_device(const Csc& g, bool full_padding, cudaStream_t s, DeviceBv
     uint64_t distinct = 0;
     for (uint32_t r = 0; r < R; ++r) distinct += hu[r];
     out.no_padded = S - distinct;  // every distinct row's slice has a non-zero mask
+}
+
+void compact_tiles_device(const uint32_t* row_ids, const uint32_t* masks, const uint32_t* rset_tile, uint32_t R,
+                          cudaStream_t s, CompactTiles& out) {
+    int dev = 0, sms = 0;
+    BLEST_CUDA(cudaGetDevice(&dev));
+    BLEST_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    Scratch tmp;
+    uint32_t* tiles = tmp.get<uint32_t>((size_t)R + 1);
+    dev::compact_count_kernel<<<sms * 8, 256, 0, s>>>(masks, rset_tile, R, tiles);
+    BLEST_CUDA(cudaGetLastError());
+    out = CompactTiles{};
+    out.rset_tile = dmalloc<uint32_t>((size_t)R + 1);
+    try {
+        exclusive_scan(tiles, out.rset_tile, R + 1, s);
+        uint32_t T = 0;
+        BLEST_CUDA(cudaMemcpy(&T, out.rset_tile + R, 4, cudaMemcpyDeviceToHost));
+        out.tiles = T;
+        out.row_ids = dmalloc<uint32_t>(4ull * T);
+        out.masks = dmalloc<uint32_t>(T);
+        BLEST_CUDA(cudaMemsetAsync(out.row_ids, 0xFF, 16ull * T, s));
+        BLEST_CUDA(cudaMemsetAsync(out.masks, 0, 4ull * T, s));
+        dev::compact_fill_kernel<<<sms * 8, 256, 0, s>>>((const uint4*)row_ids, masks, rset_tile, out.rset_tile, R,
+                                                         out.row_ids, (uint8_t*)out.masks);
+        BLEST_CUDA(cudaGetLastError());
+        BLEST_CUDA(cudaStreamSynchronize(s));
+    } catch (...) {
+        cudaFree(out.rset_tile);
+        cudaFree(out.row_ids);
+        cudaFree(out.masks);
+        out = CompactTiles{};
+        throw;
+    }
 }
 
 void device_bvss_free(DeviceBvss& b) {

@@ -19,20 +19,20 @@ constexpr uint64_t kQUnitMask = (1ull << kQShift) - 1;
 // Grid barrier wait bound (nanoseconds of %globaltimer).
 constexpr uint64_t kBarrierTimeoutNs = 2000000000ull;
 
-// Graph as resident in HBM. BVSS arrays keep the reference layout
-// (BVSS.cuh:87-91); rset_tile is derived at upload: tiles of real slice
-// set r are [rset_tile[r], rset_tile[r+1]) (tile = 4 slices = one uint4
-// of row ids + one 32-bit mask word).
+// Graph as resident in HBM. The BVSS (BVSS.cuh:87-91) is kept as the
+// kernels read it: per real slice set r, its non-empty slices (row id +
+// mask byte, in BVSS order) packed 4 per tile in tiles [rset_tile[r],
+// rset_tile[r+1]) (tile = one uint4 of row ids + one 32-bit mask word; the
+// rset's last tile padded with row 0xFFFFFFFF / mask 0). Without full
+// padding that is the BVSS's own slice array; with full padding (75 % empty
+// slices on a grid) it is a quarter of it. The vset arrays are not needed
+// on the device.
 struct DevGraph {
     uint32_t n;
     uint32_t no_real;
-    uint32_t no_virtual;
     uint32_t nnz;
-    uint64_t no_slices;
+    uint64_t no_slices;         // 4 * tiles
     uint64_t degree_total;      // sum of CSR degrees
-    const uint64_t* slice_set_ptrs;
-    const uint32_t* virtual_to_real;
-    const uint32_t* real_ptrs;
     const uint4* row4;          // row ids, 4 per tile
     const uint32_t* masks;      // one word per tile
     const uint32_t* rset_tile;  // R + 1

@@ -868,26 +868,21 @@ T* plan_alloc(blest_graph* u, size_t count) {
 void join_graphs(const std::vector<const blest_graph*>& gs, const std::vector<uint32_t>& off, uint32_t N,
                  blest_graph* u, cudaStream_t s) {
     using dev::JoinSeg;
-    uint64_t V = 0, T = 0, E = 0, C = 0;
+    uint64_t T = 0, E = 0, C = 0;
     for (auto* g : gs) {
-        V += g->d.no_virtual;
         T += g->d.no_slices / 4;
         E += g->d.nnz;
         C += g->d.no_pull_chunks;
     }
-    if (V >= 0xFFFFFFFFull || T >= 0xFFFFFFFFull || E >= 0xFFFFFF00ull || C >= 0xFFFFFFFFull)
-        throw Error(BLEST_ERR_UNSUPPORTED, "joined graph exceeds 2^32 vertex sets, tiles or edges");
+    if (T >= 0xFFFFFFFFull || E >= 0xFFFFFF00ull || C >= 0xFFFFFFFFull)
+        throw Error(BLEST_ERR_UNSUPPORTED, "joined graph exceeds 2^32 tiles or edges");
     const uint32_t R = N / 8;
     dev::DevGraph& d = u->d;
     d.n = N;
     d.no_real = R;
-    d.no_virtual = (uint32_t)V;
     d.no_slices = 4 * T;
     d.nnz = (uint32_t)E;
     d.degree_total = E;
-    uint64_t* ssp = plan_alloc<uint64_t>(u, V + 1);
-    uint32_t* v2r = plan_alloc<uint32_t>(u, V);
-    uint32_t* rp = plan_alloc<uint32_t>(u, (size_t)R + 1);
     uint32_t* rows = plan_alloc<uint32_t>(u, 4 * T);
     uint32_t* masks = plan_alloc<uint32_t>(u, T);
     uint32_t* rt = plan_alloc<uint32_t>(u, (size_t)R + 1);
@@ -899,15 +894,11 @@ void join_graphs(const std::vector<const blest_graph*>& gs, const std::vector<ui
     auto seg = [&](const void* src, void* dst, uint64_t count, uint64_t add, uint32_t kind) {
         if (count) segs.push_back(JoinSeg{src, dst, count, add, kind, 0});
     };
-    uint64_t vo = 0, to = 0, eo = 0, co = 0;
+    uint64_t to = 0, eo = 0, co = 0;
     for (size_t i = 0; i < gs.size(); ++i) {
         const dev::DevGraph& g = gs[i]->d;
         const uint32_t o = off[i], ri = g.no_real, rpad = (o + ((g.n + 31) & ~31u)) / 8 - o / 8;
         const uint64_t ti = g.no_slices / 4;
-        seg(g.slice_set_ptrs, ssp + vo, g.no_virtual, 4 * to, dev::kAdd64);
-        seg(g.virtual_to_real, v2r + vo, g.no_virtual, o / 8, dev::kAdd32);
-        seg(g.real_ptrs, rp + o / 8, ri, vo, dev::kAdd32);
-        seg(nullptr, rp + o / 8 + ri, rpad - ri, vo + g.no_virtual, dev::kFill32);
         seg(g.row4, rows + 4 * to, 4 * ti, o, dev::kAdd32KeepPad);
         seg(g.masks, masks + to, ti, 0, dev::kAdd32);
         seg(g.rset_tile, rt + o / 8, ri, to, dev::kAdd32);
@@ -918,13 +909,10 @@ void join_graphs(const std::vector<const blest_graph*>& gs, const std::vector<ui
         if (g.has_in) seg(g.has_in, hin + o / 32, (g.n + 31) / 32, 0, dev::kAdd32);
         else seg(nullptr, hin + o / 32, (g.n + 31) / 32, 0xFFFFFFFFull, dev::kFill32);
         seg(g.pull_chunks, pieces + co, g.no_pull_chunks, (uint64_t)o | (eo << 32), dev::kPiece);
-        vo += g.no_virtual;
         to += ti;
         eo += g.nnz;
         co += g.no_pull_chunks;
     }
-    seg(nullptr, ssp + V, 1, 4 * T, dev::kFill64);
-    seg(nullptr, rp + R, 1, V, dev::kFill32);
     seg(nullptr, rt + R, 1, T, dev::kFill32);
     seg(nullptr, cp + N, 1, E, dev::kFill32);
     seg(nullptr, hin + N / 32, 4, 0, dev::kFill32);
@@ -940,9 +928,6 @@ void join_graphs(const std::vector<const blest_graph*>& gs, const std::vector<ui
     BLEST_CUDA(e1);
     BLEST_CUDA(cudaGetLastError());
     BLEST_CUDA(e2);
-    d.slice_set_ptrs = ssp;
-    d.virtual_to_real = v2r;
-    d.real_ptrs = rp;
     d.row4 = (const uint4*)rows;
     d.masks = masks;
     d.rset_tile = rt;

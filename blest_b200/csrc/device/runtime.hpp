@@ -65,6 +65,8 @@ struct blest_graph {
     int device = 0;
     int sm_count = 0;
     blest::dev::DevGraph d{};
+    uint32_t bvss_virtual = 0;  // the BVSS's vsets and slices (reported by info)
+    uint64_t bvss_slices = 0;
     std::vector<void*> allocations;
     uint64_t graph_bytes = 0;
     uint64_t undirected_edges = 0;
@@ -131,6 +133,19 @@ struct DeviceBvss {
 };
 void bvss_build_device(const Csc& g, bool full_padding, cudaStream_t s, DeviceBvss& out);
 void device_bvss_free(DeviceBvss& b);
+
+// The tiles the kernels read: each rset's non-empty slices (mask != 0) in
+// BVSS order, 4 per tile, the rset's last tile padded; rset_tile[r] = the
+// rset's first tile. Built on the device from a BVSS's rows/masks and its
+// rset tile table (all device pointers; outputs owned by the caller).
+struct CompactTiles {
+    uint32_t tiles = 0;
+    uint32_t* row_ids = nullptr;  // 4 * tiles
+    uint32_t* masks = nullptr;    // tiles
+    uint32_t* rset_tile = nullptr;  // R + 1
+};
+void compact_tiles_device(const uint32_t* row_ids, const uint32_t* masks, const uint32_t* rset_tile, uint32_t R,
+                          cudaStream_t s, CompactTiles& out);
 void mbfs_scratch_free(void* p);
 // Allocate the multi-source BFS state of `words` 32-bit words per vertex now.
 void mbfs_reserve(Workspace& w, uint32_t n, uint32_t words);

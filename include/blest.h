@@ -206,6 +206,8 @@ typedef struct blest_graph_info {
     uint64_t device_bytes_graph;     /* resident structure */
     uint64_t device_bytes_workspace; /* one BFS/CC workspace */
     int device;
+    uint64_t device_tiles;           /* tiles the kernels read: the BVSS's non-empty
+                                        slices, 4 per tile, per real slice set */
 } blest_graph_info;
 
 /* Uploads the BVSS and CSR once; the graph stays resident until destroy.

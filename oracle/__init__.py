@@ -220,6 +220,12 @@ def rlib():
         lib.ref_cc.argtypes = [vp, P32, C.POINTER(C.c_double), P32]
         lib.ref_cc_raw.argtypes = [vp, P32, C.POINTER(C.c_double)]
         lib.ref_destroy.argtypes = [vp]
+        lib.ref_csc_save.argtypes = [vp, C.c_char_p]
+        lib.ref_csc_load.argtypes = [C.c_char_p, C.POINTER(vp)]
+        lib.ref_ordering_save.argtypes = [vp, C.c_char_p, P32]
+        lib.ref_ordering_load.argtypes = [vp, C.c_char_p, P32]
+        lib.ref_bvss_save.argtypes = [vp, C.c_char_p]
+        lib.ref_bvss_load.argtypes = [C.c_char_p, C.POINTER(vp)]
         _rlib = lib
     return _rlib
 
@@ -258,6 +264,36 @@ class RefGraph:
                                             _p64(ssp), _p32(v2r), _p32(rp), _p32(ri), _p32(mk), ci.size,
                                             _p32(cp), _p32(ci), C.byref(h)))
         return cls(h)
+
+    @classmethod
+    def load_csc(cls, path) -> "RefGraph":
+        """CSC::constructFromBinary of a _csc.bin file."""
+        h = C.c_void_p()
+        _rcheck(rlib().ref_csc_load(str(path).encode(), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def load_bvss(cls, path) -> "RefGraph":
+        """BVSS::constructFromBinary of a _bvss.bin file."""
+        h = C.c_void_p()
+        _rcheck(rlib().ref_bvss_load(str(path).encode(), C.byref(h)))
+        return cls(h)
+
+    def save_csc(self, path) -> None:
+        _rcheck(rlib().ref_csc_save(self.h, str(path).encode()))
+
+    def save_ordering(self, path, inv) -> None:
+        _rcheck(rlib().ref_ordering_save(self.h, str(path).encode(), _p32(_u32(inv))))
+
+    def load_ordering(self, path) -> np.ndarray:
+        """CSC::orderFromBinary: read and apply; returns the permutation."""
+        n = self.csc()[0]
+        inv = np.empty(n, dtype=np.uint32)
+        _rcheck(rlib().ref_ordering_load(self.h, str(path).encode(), _p32(inv)))
+        return inv
+
+    def save_bvss(self, path) -> None:
+        _rcheck(rlib().ref_bvss_save(self.h, str(path).encode()))
 
     def is_social(self) -> bool:
         s = C.c_int()

@@ -341,6 +341,54 @@ int ref_cc_raw(void* h, uint32_t* labels_out, double* seconds) {
     });
 }
 
+/* The reference's own cache writers and readers (CSC.cuh:225-266,
+ * :335-356; BVSS.cuh:125-183), for interchange tests in both directions. */
+int ref_csc_save(void* h, const char* path) {
+    return guard([&] { ((RefGraph*)h)->csc->saveToBinary(path); });
+}
+
+int ref_csc_load(const char* path, void** out) {
+    return guard([&] {
+        StdoutToStderr redirect;
+        CSC* c = new CSC;
+        c->constructFromBinary(path);
+        RefGraph* g = new RefGraph;
+        g->csc = c;
+        *out = g;
+    });
+}
+
+int ref_ordering_save(void* h, const char* path, const uint32_t* inv) {
+    return guard([&] { ((RefGraph*)h)->csc->saveOrderingToBinary(path, const_cast<unsigned*>(inv)); });
+}
+
+/* CSC::orderFromBinary: reads the permutation and applies it to the CSC. */
+int ref_ordering_load(void* h, const char* path, uint32_t* inv_out) {
+    return guard([&] {
+        StdoutToStderr redirect;
+        CSC* c = ((RefGraph*)h)->csc;
+        unsigned* inv = c->orderFromBinary(path);
+        std::memcpy(inv_out, inv, 4ull * c->getN());
+        delete[] inv;
+    });
+}
+
+int ref_bvss_save(void* h, const char* path) {
+    return guard([&] { ((RefGraph*)h)->bvss->saveToBinary(path); });
+}
+
+int ref_bvss_load(const char* path, void** out) {
+    return guard([&] {
+        StdoutToStderr redirect;
+        BVSS* b = new BVSS(8, 4, null_stream());
+        b->m_CSR = nullptr;  // the constructor leaves it unset; a loaded BVSS has none
+        b->constructFromBinary(path);
+        RefGraph* g = new RefGraph;
+        g->bvss = b;
+        *out = g;
+    });
+}
+
 int ref_destroy(void* h) {
     RefGraph* g = (RefGraph*)h;
     if (!g) return 0;
