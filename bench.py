@@ -55,6 +55,10 @@ WORKLOADS = {
                     "multi-source BFS, RMAT scale 20 ef 16, Jaccard window 65536, 128 seeded sources (one group; "
                     "the profiling case)"),
     "cc_rmat20": ("cc", ("rmat", 20, 16), "jaccard", 65536, 0, "connected components, RMAT scale 20 (profiling case)"),
+    "er23": ("bfs", ("er", 23, 32), "rcm", 0, 32,
+             "Erdos-Renyi 2^23 vertices avg degree 32, RCM, 32 sources (profiling case of er25)"),
+    "grid2048": ("bfs", ("grid", 2048, 2048), "rcm", 0, 32,
+                 "2D 2048x2048 grid, 5% edges deleted, 0.1% shortcuts, RCM, 32 sources (profiling case of grid4096)"),
     "mbfs_rmat22": ("mbfs", ("rmat", 22, 16), "jaccard", 65536, 1024,
                     "multi-source BFS, RMAT scale 22 ef 16, Jaccard window 65536, 1024 seeded sources "
                     "in bit-packed groups of 128"),

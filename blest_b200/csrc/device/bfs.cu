@@ -173,44 +173,67 @@ __device__ __forceinline__ void flush_enqueue(const BfsArgs& a, Enqueue& q, int 
     q.units = 0;
 }
 
-// Claim vertex `row` for `level`; the atomicOr on visited decides the
-// single winner, which records level/parent, sets the frontier bit and,
-// when it is the first new vertex of its rset this level, queues the rset.
-// `precheck`: read the visited word first and skip the atomic for visited
-// rows (saves contended atomics in big levels; small levels skip the read,
-// one round trip less on their critical path).
+// The hit slices of one tile (bit k of `hits` = slice k, row rowk[k]),
+// claimed together: the visited atomics of all of them are in flight at
+// once, then the frontier atomics of the winners; each winner records its
+// level (and parent: the first frontier column of its slice's mask, in
+// rset src_r), and queues its rset when it is the rset's first new vertex
+// this level. A tile of a dense BVSS (4 non-empty slices) thus costs two
+// round trips instead of four dependent claim chains.
 template <bool ALIGNED, bool PARENTS>
-__device__ __forceinline__ void discover(const BfsArgs& a, uint32_t* fcur, uint32_t* fsum, uint32_t row,
-                                         uint32_t parent, uint32_t level, Enqueue& q, uint32_t& disc,
-                                         uint64_t& deg, bool precheck) {
-    if (row >= a.g.n) {
-        set_error(a.ctr, BLEST_ERR_DEVICE_INDEX);
-        return;
+__device__ __forceinline__ void discover4(const BfsArgs& a, uint32_t* fcur, uint32_t* fsum, const uint32_t (&rowk)[4],
+                                          uint32_t hits, uint32_t mask, uint32_t fb, uint32_t src_r, uint32_t level,
+                                          Enqueue& q, uint32_t& disc, uint64_t& deg, bool precheck) {
+    uint32_t got[4];
+#pragma unroll
+    for (uint32_t k = 0; k < 4; ++k) {
+        got[k] = 0xFFFFFFFFu;
+        if (((hits >> k) & 1u) && rowk[k] >= a.g.n) {
+            set_error(a.ctr, BLEST_ERR_DEVICE_INDEX);
+            hits &= ~(1u << k);
+        }
     }
-    const uint32_t w = row >> 5, b = 1u << (row & 31);
-    if (precheck && (__ldcg(&a.visited[w]) & b)) return;
-    const uint32_t old = atomicOr(&a.visited[w], b);
-    if (old & b) return;
-    a.levels[row] = level;
-    if (PARENTS) a.parents[row] = parent;
-    ++disc;
-    // degree and rset tile bounds are loaded together with the frontier
-    // atomic (one round trip instead of three)
-    const uint32_t r = row >> 3;
-    const uint32_t d0 = __ldg(&a.g.csr_ptrs[row]), d1 = __ldg(&a.g.csr_ptrs[row + 1]);
-    const uint32_t t0 = __ldg(&a.g.rset_tile[r]), t1 = __ldg(&a.g.rset_tile[r + 1]);
-    const uint32_t oldF = atomicOr(&fcur[w], b);
-    deg += d1 - d0;
-    if (((oldF >> (row & 24)) & 0xFFu) == 0) {
-        const uint32_t units = ALIGNED ? (t1 - t0 + 31) / 32 : t1 - t0;
-        if (units) {
-            q.rset[q.cnt++] = r;
-            q.units += units;
-            summary_set(a, fsum, w);
+    if (precheck) {
+#pragma unroll
+        for (uint32_t k = 0; k < 4; ++k)
+            if ((hits >> k) & 1u) got[k] = __ldcg(&a.visited[rowk[k] >> 5]);
+#pragma unroll
+        for (uint32_t k = 0; k < 4; ++k)
+            if (((hits >> k) & 1u) && ((got[k] >> (rowk[k] & 31)) & 1u)) hits &= ~(1u << k);
+    }
+#pragma unroll
+    for (uint32_t k = 0; k < 4; ++k)
+        if ((hits >> k) & 1u) got[k] = atomicOr(&a.visited[rowk[k] >> 5], 1u << (rowk[k] & 31));
+    uint32_t won = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < 4; ++k)
+        if (((hits >> k) & 1u) && !((got[k] >> (rowk[k] & 31)) & 1u)) won |= 1u << k;
+    if (!won) return;
+#pragma unroll
+    for (uint32_t k = 0; k < 4; ++k) {
+        if (!((won >> k) & 1u)) continue;
+        const uint32_t row = rowk[k];
+        a.levels[row] = level;
+        if (PARENTS) a.parents[row] = src_r * 8 + (__ffs((mask >> (8 * k)) & fb & 0xFFu) - 1);
+        got[k] = atomicOr(&fcur[row >> 5], 1u << (row & 31));
+    }
+#pragma unroll
+    for (uint32_t k = 0; k < 4; ++k) {
+        if (!((won >> k) & 1u)) continue;
+        const uint32_t row = rowk[k];
+        ++disc;
+        deg += __ldg(&a.g.csr_ptrs[row + 1]) - __ldg(&a.g.csr_ptrs[row]);
+        if (((got[k] >> (row & 24)) & 0xFFu) == 0) {
+            const uint32_t r = row >> 3;
+            const uint32_t units = rset_units<ALIGNED>(a.g, r);
+            if (units) {
+                q.rset[q.cnt++] = r;
+                q.units += units;
+                summary_set(a, fsum, row >> 5);
+            }
         }
     }
 }
-
 
 // One push step's operands: the tile of this lane (row ids, mask word),
 // the frontier byte of its rset, and the queue owner of the next step.
@@ -509,22 +532,23 @@ __device__ __forceinline__ void bfs_run(const BfsArgs& a) {
                     }
                     if (hits) {
                         const uint32_t rowk[4] = {cur.rows.x, cur.rows.y, cur.rows.z, cur.rows.w};
+                        if (lazy) {
+                            // the hit rows' visited words first (independent
+                            // loads in flight together), then the ORs
+                            uint32_t vis[4];
 #pragma unroll
-                        for (uint32_t kk = 0; kk < 4; ++kk) {
-                            if (hits & (1u << kk)) {
-                                const uint32_t hb = (cur.mask >> (8 * kk)) & cur.fb & 0xFFu;
+                            for (uint32_t kk = 0; kk < 4; ++kk)
+                                vis[kk] = ((hits >> kk) & 1u) && rowk[kk] < g.n ? __ldcg(&a.visited[rowk[kk] >> 5]) : 0u;
+#pragma unroll
+                            for (uint32_t kk = 0; kk < 4; ++kk) {
+                                if (!((hits >> kk) & 1u)) continue;
                                 const uint32_t row = rowk[kk];
-                                if (lazy) {
-                                    if (row >= g.n) {
-                                        set_error(c, BLEST_ERR_DEVICE_INDEX);
-                                    } else if (!((__ldcg(&a.visited[row >> 5]) >> (row & 31)) & 1u)) {
-                                        atomicOr(&fcur[row >> 5], 1u << (row & 31));
-                                    }
-                                } else {
-                                    discover<ALIGNED, PARENTS>(a, fcur, fsum, row, cur.r * 8 + (__ffs(hb) - 1), level, q,
-                                                               disc, deg, precheck);
-                                }
+                                if (row >= g.n) set_error(c, BLEST_ERR_DEVICE_INDEX);
+                                else if (!((vis[kk] >> (row & 31)) & 1u)) atomicOr(&fcur[row >> 5], 1u << (row & 31));
                             }
+                        } else {
+                            discover4<ALIGNED, PARENTS>(a, fcur, fsum, rowk, hits, cur.mask, cur.fb, cur.r, level, q,
+                                                        disc, deg, precheck);
                         }
                     }
                     flush_enqueue<ALIGNED>(a, q, kEnqueueCap - 4);
