@@ -516,40 +516,53 @@ __device__ __forceinline__ void bfs_run(const BfsArgs& a) {
             const uint32_t k = (steps + nwarps - 1) / nwarps;
             uint32_t s = warp * k;
             const uint32_t send = min(steps, s + k);
-            if (s < send) {
+            auto tile_hits = [&](const StepLoad& t) -> uint32_t {
+                if (MMA) return hits_mma(t.mask, t.fb);
+                uint32_t h = 0;
+#pragma unroll
+                for (uint32_t kk = 0; kk < 4; ++kk) h |= (((t.mask >> (8 * kk)) & t.fb & 0xFFu) ? 1u : 0u) << kk;
+                return h;
+            };
+            if (s < send && lazy) {
+                // Lazy levels claim nothing and queue nothing, which leaves
+                // registers to software-pipeline the steps: the loads of
+                // step s + 1 (queue entry, tile range, tile) are in flight
+                // while step s's hit rows are checked and ORed.
+                StepLoad cur = load_step<ALIGNED>(a, fprev, find_owner(a.q_off, E2, E1, U2 + s * per), E1, U1,
+                                                  U2 + s * per, c);
+                for (; s < send; ++s) {
+                    const bool more = s + 1 < send;  // warp-uniform
+                    StepLoad nxt;
+                    if (more) nxt = load_step<ALIGNED>(a, fprev, cur.next_owner, E1, U1, U2 + (s + 1) * per, c);
+                    const uint32_t hits = tile_hits(cur);
+                    if (hits) {
+                        const uint32_t rowk[4] = {cur.rows.x, cur.rows.y, cur.rows.z, cur.rows.w};
+                        // the hit rows' visited words first (independent loads
+                        // in flight together), then the ORs
+                        uint32_t vis[4];
+#pragma unroll
+                        for (uint32_t kk = 0; kk < 4; ++kk)
+                            vis[kk] = ((hits >> kk) & 1u) && rowk[kk] < g.n ? __ldcg(&a.visited[rowk[kk] >> 5]) : 0u;
+#pragma unroll
+                        for (uint32_t kk = 0; kk < 4; ++kk) {
+                            if (!((hits >> kk) & 1u)) continue;
+                            const uint32_t row = rowk[kk];
+                            if (row >= g.n) set_error(c, BLEST_ERR_DEVICE_INDEX);
+                            else if (!((vis[kk] >> (row & 31)) & 1u)) atomicOr(&fcur[row >> 5], 1u << (row & 31));
+                        }
+                    }
+                    if (more) cur = nxt;
+                }
+            } else if (s < send) {
                 uint32_t owner = find_owner(a.q_off, E2, E1, U2 + s * per);
                 for (; s < send; ++s) {
                     const StepLoad cur = load_step<ALIGNED>(a, fprev, owner, E1, U1, U2 + s * per, c);
                     owner = cur.next_owner;
-                    uint32_t hits;
-                    if (MMA) {
-                        hits = hits_mma(cur.mask, cur.fb);
-                    } else {
-                        hits = 0;
-#pragma unroll
-                        for (uint32_t kk = 0; kk < 4; ++kk)
-                            hits |= (((cur.mask >> (8 * kk)) & cur.fb & 0xFFu) ? 1u : 0u) << kk;
-                    }
+                    const uint32_t hits = tile_hits(cur);
                     if (hits) {
                         const uint32_t rowk[4] = {cur.rows.x, cur.rows.y, cur.rows.z, cur.rows.w};
-                        if (lazy) {
-                            // the hit rows' visited words first (independent
-                            // loads in flight together), then the ORs
-                            uint32_t vis[4];
-#pragma unroll
-                            for (uint32_t kk = 0; kk < 4; ++kk)
-                                vis[kk] = ((hits >> kk) & 1u) && rowk[kk] < g.n ? __ldcg(&a.visited[rowk[kk] >> 5]) : 0u;
-#pragma unroll
-                            for (uint32_t kk = 0; kk < 4; ++kk) {
-                                if (!((hits >> kk) & 1u)) continue;
-                                const uint32_t row = rowk[kk];
-                                if (row >= g.n) set_error(c, BLEST_ERR_DEVICE_INDEX);
-                                else if (!((vis[kk] >> (row & 31)) & 1u)) atomicOr(&fcur[row >> 5], 1u << (row & 31));
-                            }
-                        } else {
-                            discover4<ALIGNED, PARENTS>(a, fcur, fsum, rowk, hits, cur.mask, cur.fb, cur.r, level, q,
-                                                        disc, deg, precheck);
-                        }
+                        discover4<ALIGNED, PARENTS>(a, fcur, fsum, rowk, hits, cur.mask, cur.fb, cur.r, level, q,
+                                                    disc, deg, precheck);
                     }
                     flush_enqueue<ALIGNED>(a, q, kEnqueueCap - 4);
                 }
