@@ -209,6 +209,7 @@ _SIGS = {
     "blest_server_add_graph": [vp, vp, P(u32)],
     "blest_server_add_virtual_graph": [vp, u32, u64, P(u32)],
     "blest_server_submit": [vp, u32, i32, u32, vp, P(u64)],
+    "blest_server_submit_ex": [vp, u32, i32, u32, vp, i32, P(u64)],
     "blest_server_poll": [vp, u64, P(i32), P(QueryResult)],
     "blest_server_wait": [vp, u64, f64, P(QueryResult)],
     "blest_server_drain": [vp, f64],

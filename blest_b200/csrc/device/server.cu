@@ -13,8 +13,9 @@
 //    BLEST_ERR_ADMISSION).
 // Each lane has its own CUDA stream and per-graph workspaces whose
 // cooperative grids are capped to a share of the SMs, so jobs on different
-// lanes run side by side on the device. Results land in the caller's host
-// buffer; each request records submit / start / done times.
+// lanes run side by side on the device. Results land in the caller's
+// buffer, host memory or (for a consumer on the GPU) device memory; each
+// request records submit / start / done times.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -45,6 +46,7 @@ struct Request {
     int kind = BLEST_QUERY_BFS;
     uint32_t source = 0;
     uint32_t* out = nullptr;
+    int out_mem = BLEST_MEM_HOST;  // where `out` lives
     int status = BLEST_OK;
     uint32_t batch = 0;
     double submit = 0, start = 0, done_t = 0;
@@ -149,15 +151,18 @@ int run_job(blest_server* s, Lane& lane, Job& job) {
     }
     blest_workspace* ws = lane.ws[job.graph];
     if (job.kind == BLEST_QUERY_CC) {
-        int rc = blest_cc_ws(ws, job.reqs[0]->out, BLEST_MEM_HOST, lane.stream, nullptr);
+        const Request& r0 = *job.reqs[0];
+        int rc = blest_cc_ws(ws, r0.out, r0.out_mem, lane.stream, nullptr);
         if (rc != BLEST_OK) return rc;
-        for (size_t i = 1; i < job.reqs.size(); ++i)
-            std::memcpy(job.reqs[i]->out, job.reqs[0]->out, 4ull * ge.n);
-        return BLEST_OK;
+        for (size_t i = 1; i < job.reqs.size() && rc == BLEST_OK; ++i)
+            if (cudaMemcpyAsync(job.reqs[i]->out, r0.out, 4ull * ge.n, cudaMemcpyDefault, lane.stream) != cudaSuccess)
+                rc = BLEST_ERR_CUDA;
+        if (cudaStreamSynchronize(lane.stream) != cudaSuccess && rc == BLEST_OK) rc = BLEST_ERR_CUDA;
+        return rc;
     }
     if (job.reqs.size() == 1)
-        return blest_bfs_ws(ws, job.reqs[0]->source, job.reqs[0]->out, nullptr, BLEST_MEM_HOST, nullptr, lane.stream,
-                            0, nullptr);
+        return blest_bfs_ws(ws, job.reqs[0]->source, job.reqs[0]->out, nullptr, job.reqs[0]->out_mem, nullptr,
+                            lane.stream, 0, nullptr);
     const uint32_t k = (uint32_t)job.reqs.size();
     std::vector<uint32_t> src(k);
     for (uint32_t i = 0; i < k; ++i) src[i] = job.reqs[i]->source;
@@ -171,7 +176,7 @@ int run_job(blest_server* s, Lane& lane, Job& job) {
     int rc = blest_mbfs_ws(ws, src.data(), k, staging, BLEST_MEM_DEVICE, &mp, lane.stream, nullptr);
     if (rc == BLEST_OK) {
         for (uint32_t i = 0; i < k && rc == BLEST_OK; ++i)
-            if (cudaMemcpyAsync(job.reqs[i]->out, staging + (size_t)i * ge.n, 4ull * ge.n, cudaMemcpyDeviceToHost,
+            if (cudaMemcpyAsync(job.reqs[i]->out, staging + (size_t)i * ge.n, 4ull * ge.n, cudaMemcpyDefault,
                                 lane.stream) != cudaSuccess)
                 rc = BLEST_ERR_CUDA;
     }
@@ -358,9 +363,16 @@ int blest_server_add_virtual_graph(blest_server* s, uint32_t n, uint64_t nnz, ui
 
 int blest_server_submit(blest_server* s, uint32_t graph_id, int kind, uint32_t source, uint32_t* out_host,
                         uint64_t* ticket) {
+    return blest_server_submit_ex(s, graph_id, kind, source, out_host, BLEST_MEM_HOST, ticket);
+}
+
+int blest_server_submit_ex(blest_server* s, uint32_t graph_id, int kind, uint32_t source, uint32_t* out, int out_mem,
+                           uint64_t* ticket) {
     return guarded([&] {
-        blest::require(s && ticket && out_host, "null argument");
+        blest::require(s && ticket && out, "null argument");
         blest::require(kind == BLEST_QUERY_BFS || kind == BLEST_QUERY_CC, "bad query kind");
+        blest::require(out_mem == BLEST_MEM_HOST || out_mem == BLEST_MEM_DEVICE, "bad out_mem");
+        blest::require(!(s->p.dry_run && out_mem == BLEST_MEM_DEVICE), "dry-run servers take host buffers only");
         std::lock_guard<std::mutex> lk(s->mu);
         blest::require(graph_id < s->graphs.size(), "unknown graph id");
         if (kind == BLEST_QUERY_BFS && source >= s->graphs[graph_id].n)
@@ -371,7 +383,8 @@ int blest_server_submit(blest_server* s, uint32_t graph_id, int kind, uint32_t s
         r->graph = graph_id;
         r->kind = kind;
         r->source = source;
-        r->out = out_host;
+        r->out = out;
+        r->out_mem = out_mem;
         r->submit = blest::now(s);
         s->pending.push_back(r.get());
         *ticket = r->id;

@@ -91,16 +91,24 @@ class Server:
         g = self._graphs.get(gid, 1)  # unknown ids are refused by the library
         return g if isinstance(g, int) else g.n
 
-    def _submit(self, gid: int, kind: int, source: int, out: np.ndarray | None = None) -> Ticket:
+    def _submit(self, gid: int, kind: int, source: int, out=None) -> Ticket:
         if out is None:
             out = np.empty(self._n(gid), dtype=np.uint32)
-        assert out.dtype == np.uint32 and out.size >= self._n(gid) and out.flags.c_contiguous
         t = L.u64()
-        L.call("blest_server_submit", self._h, gid, kind, source, out.ctypes.data, C.byref(t))
+        if isinstance(out, np.ndarray):
+            assert out.dtype == np.uint32 and out.size >= self._n(gid) and out.flags.c_contiguous
+            L.call("blest_server_submit_ex", self._h, gid, kind, source, out.ctypes.data, L.MEM_HOST, C.byref(t))
+        else:
+            # a device buffer (a CUDA tensor of >= n 4-byte elements): the
+            # result stays on the GPU
+            assert out.is_cuda and out.is_contiguous() and out.element_size() == 4 and out.numel() >= self._n(gid)
+            L.call("blest_server_submit_ex", self._h, gid, kind, source, out.data_ptr(), L.MEM_DEVICE, C.byref(t))
         return Ticket(self, t.value, out)
 
-    def submit_bfs(self, gid: int, source: int, out: np.ndarray | None = None) -> Ticket:
-        """`out`: optional uint32[n] result buffer (e.g. pinned memory)."""
+    def submit_bfs(self, gid: int, source: int, out=None) -> Ticket:
+        """`out`: optional result buffer, a uint32[n] numpy array (e.g. pinned
+        memory) or a CUDA tensor of n int32/uint32 (the result stays on the
+        device)."""
         return self._submit(gid, L.QUERY_BFS, source, out)
 
     def submit_cc(self, gid: int, out: np.ndarray | None = None) -> Ticket:

@@ -505,6 +505,11 @@ int blest_server_add_graph(blest_server* s, blest_graph* g, uint32_t* graph_id);
 int blest_server_add_virtual_graph(blest_server* s, uint32_t n, uint64_t nnz, uint32_t* graph_id);
 int blest_server_submit(blest_server* s, uint32_t graph_id, int kind, uint32_t source, uint32_t* out_host,
                         uint64_t* ticket);
+/* Same with the result buffer in host (BLEST_MEM_HOST) or device memory
+ * (BLEST_MEM_DEVICE, on the server's device: the result stays in HBM for a
+ * consumer on the GPU and no host copy is made). */
+int blest_server_submit_ex(blest_server* s, uint32_t graph_id, int kind, uint32_t source, uint32_t* out, int out_mem,
+                           uint64_t* ticket);
 int blest_server_poll(blest_server* s, uint64_t ticket, int* done, blest_query_result* result);
 int blest_server_wait(blest_server* s, uint64_t ticket, double timeout_s, blest_query_result* result);
 /* Wait until every submitted request has finished or been refused. */

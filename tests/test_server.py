@@ -121,6 +121,35 @@ def test_results_equal_alone_and_in_the_mix(gpu):
 
 
 @pytest.mark.gpu
+def test_device_results_equal_host_results(gpu):
+    """Results written to device buffers (for a consumer on the GPU) equal
+    the oracle's, alone and coalesced, for BFS and CC."""
+    import torch
+    import oracle as O
+    from blest_b200 import Csc, Graph
+    from graphs import prepared
+    csc, bvss, csr = prepared(Csc.rmat(13, 16, seed=4, permute_seed=1), "jaccard", 4096)
+    g = Graph(bvss, csr)
+    srv = Server(lanes=2, max_batch=32)
+    gid = srv.add_graph(g)
+    srcs = [int(x) for x in csc.sample_sources(40, seed=3)]
+    outs = [torch.empty(csc.n, dtype=torch.int32, device="cuda") for _ in srcs]
+    tickets = [srv.submit_bfs(gid, s, out=o) for s, o in zip(srcs, outs)]
+    cc_out = torch.empty(csc.n, dtype=torch.int32, device="cuda")
+    tc = srv.submit_cc(gid, out=cc_out)
+    srv.drain(60)
+    batched = 0
+    for s, o, t in zip(srcs, outs, tickets):
+        assert t.info().status == 0
+        batched += t.info().batch_size > 1
+        np.testing.assert_array_equal(o.cpu().numpy().view(np.uint32), O.bfs_csc(csc.n, csc.col_ptrs, csc.rows, s))
+    assert batched > 0
+    assert tc.info().status == 0
+    np.testing.assert_array_equal(cc_out.cpu().numpy().view(np.uint32), O.cc_csc(csc.n, csc.col_ptrs, csc.rows))
+    srv.close()
+
+
+@pytest.mark.gpu
 def test_request_that_never_fits_is_refused(gpu):
     from blest_b200 import Csc, Graph
     from graphs import prepared
