@@ -686,16 +686,76 @@ def run_serving(args, rank, world):
         del lv
         graphs.append((name, csc, g, np.array(mr, dtype=np.int64), srcs))
         log(f"[serving] {name}: n={csc.n} nnz={csc.nnz} ({time.time() - t0:.1f}s)")
-    # pinned result buffers, recycled once a result has been consumed
+    # result buffers, recycled once a result has been consumed: pinned host
+    # memory (the result crosses PCIe) or device memory (it stays in HBM for
+    # a consumer on the GPU)
     import queue as qmod
-    pools = []
-    for _, csc, _, _, _ in graphs:
-        q = qmod.Queue()
-        # at most ~2 GB of pinned result buffers per graph
-        for _ in range(max(8, min(args.buffers, int(2e9 // (4 * csc.n))))):
-            q.put(torch.empty(csc.n, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32))
-        pools.append(q)
+
+    def make_pools(device: bool):
+        pools = []
+        for _, csc, _, _, _ in graphs:
+            q = qmod.Queue()
+            # at most ~2 GB of result buffers per graph
+            for _ in range(max(8, min(args.buffers, int(2e9 // (4 * csc.n))))):
+                if device:
+                    q.put(torch.empty(csc.n, dtype=torch.int32, device="cuda"))
+                else:
+                    q.put(torch.empty(csc.n, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32))
+            pools.append(q)
+        return pools
+
+    # parity through the server: one BFS and one CC request per graph
+    # against the oracle (outside the sweep)
+    parity = None
+    if not args.skip_check:
+        import oracle as O
+        srv = Server(lanes=args.lanes, max_batch=128)
+        bad = 0
+        for name, csc, g, _, srcs in graphs:
+            gid = srv.add_graph(g)
+            s0 = int(srcs[0])
+            tb, tc = srv.submit_bfs(gid, s0), srv.submit_cc(gid)
+            if not np.array_equal(tb.result(600), O.bfs_csc(csc.n, csc.col_ptrs, csc.rows, s0)):
+                bad += 1
+                log(f"[parity] serving BFS on {name} differs from the oracle")
+            if not np.array_equal(tc.result(600), O.cc_csc(csc.n, csc.col_ptrs, csc.rows)):
+                bad += 1
+                log(f"[parity] serving CC on {name} differs from the oracle")
+        srv.close()
+        parity = {"requests_checked": 2 * len(graphs), "mismatches": bad,
+                  "against": "oracle bfs_csc / cc_csc, one BFS and one CC request per graph"}
+        if bad:
+            raise SystemExit(f"{bad} serving results differ from the oracle")
     rates = [float(r) for r in args.rates.split(",")]
+    modes = {"host": [False], "device": [True], "both": [False, True]}[args.serving_results]
+    sweeps = {}
+    for device_results in modes:
+        pools = make_pools(device_results)
+        sweeps["device" if device_results else "host"] = serving_sweep(args, graphs, pools, rates, Server)
+        del pools
+        torch.cuda.empty_cache()
+    sweep = sweeps.get("host") or sweeps["device"]
+    head = sweep[min(1, len(sweep) - 1)]
+    return {
+        "metric": "serving p50 latency (ms) at the sweep's second rate; p50/p99 and GTEPS per rate in config.sweep",
+        "value": head["p50_ms"], "unit": "ms", "n_gpus": 1, "steps": len(sweep), "warmup": 0,
+        "ms_per_step": None, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded generators; Poisson arrivals from a fixed seed)",
+        "config": {"workload": "serving",
+                   "description": (SERVING_FULL_DESCRIPTION if args.serving_full else WORKLOADS["serving"][5]),
+                   "graphs": [x[0] for x in graphs], "lanes": args.lanes, "max_batch": 128,
+                   "sweep": sweep, "sweep_device_results": sweeps.get("device"),
+                   "result_memory": "sweep: pinned host buffers (each result crosses PCIe); sweep_device_results: "
+                                    "device buffers (results stay in HBM)"},
+        "e2e": {"value": head["p50_ms"], "unit": "ms", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                "note": "latency measured from submit to result in host memory"},
+        "parity": parity,
+    }
+
+
+def serving_sweep(args, graphs, pools, rates, Server):
+    """Open-loop Poisson arrivals at each rate; returns one record per rate."""
+    import threading
     rng = np.random.default_rng(SEED)
     sweep = []
     for lam in rates:
@@ -759,18 +819,7 @@ def run_serving(args, rank, world):
                       "bfs_gteps": round(edges[0] / wall / 1e9, 3)})
         log(f"[serving] rate {lam}/s: {sweep[-1]}")
         srv.close()
-    head = sweep[min(1, len(sweep) - 1)]
-    return {
-        "metric": "serving p50 latency (ms) at the sweep's second rate; p50/p99 and GTEPS per rate in config.sweep",
-        "value": head["p50_ms"], "unit": "ms", "n_gpus": 1, "steps": len(sweep), "warmup": 0,
-        "ms_per_step": None, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-        "data": "synthetic (seeded generators; Poisson arrivals from a fixed seed)",
-        "config": {"workload": "serving",
-                   "description": (SERVING_FULL_DESCRIPTION if args.serving_full else WORKLOADS["serving"][5]),
-                   "graphs": [x[0] for x in graphs], "lanes": args.lanes, "max_batch": 128, "sweep": sweep},
-        "e2e": {"value": head["p50_ms"], "unit": "ms", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
-                "note": "latency measured from submit to result in host memory"},
-    }
+    return sweep
 
 
 def run_b200(args, rank, world):
@@ -1254,6 +1303,8 @@ def main():
     ap.add_argument("--lanes", type=int, default=4)
     ap.add_argument("--serving-full", action="store_true")
     ap.add_argument("--buffers", type=int, default=192)
+    ap.add_argument("--serving-results", choices=["host", "device", "both"], default="both",
+                    help="serving: result buffers in pinned host memory, device memory, or a sweep of each")
     ap.add_argument("--autotune", action="store_true", help="tune BFS launch parameters before timing")
     ap.add_argument("--trace-levels", type=int, default=0,
                     help="BFS: log per-level timings of this many traced runs to stderr")

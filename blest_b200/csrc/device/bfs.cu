@@ -108,6 +108,15 @@ struct Enqueue {
     uint32_t rset[kEnqueueCap];
     uint32_t cnt;
     uint32_t units;
+    // Append rset r (units u). Every access to rset[] uses a compile-time
+    // index, so the buffer stays in registers.
+    __device__ __forceinline__ void push(uint32_t r, uint32_t u) {
+#pragma unroll
+        for (uint32_t i = 0; i < kEnqueueCap; ++i)
+            if (i == cnt) rset[i] = r;
+        ++cnt;
+        units += u;
+    }
 };
 
 // Per-block state of the current level, written by thread 0 inside the
@@ -162,7 +171,9 @@ __device__ __forceinline__ void flush_enqueue(const BfsArgs& a, Enqueue& q, int 
     const uint64_t excl = base + incl - mine;
     uint32_t e = (uint32_t)(excl >> kQShift);
     uint32_t u = (uint32_t)(excl & kQUnitMask);
-    for (uint32_t i = 0; i < q.cnt; ++i) {
+#pragma unroll
+    for (uint32_t i = 0; i < kEnqueueCap; ++i) {
+        if (i >= q.cnt) break;
         const uint32_t r = q.rset[i];
         a.q_rset[e] = r;
         a.q_off[e] = u;
@@ -227,8 +238,7 @@ __device__ __forceinline__ void discover4(const BfsArgs& a, uint32_t* fcur, uint
             const uint32_t r = row >> 3;
             const uint32_t units = rset_units<ALIGNED>(a.g, r);
             if (units) {
-                q.rset[q.cnt++] = r;
-                q.units += units;
+                q.push(r, units);
                 summary_set(a, fsum, row >> 5);
             }
         }
@@ -593,8 +603,7 @@ __device__ __forceinline__ void bfs_run(const BfsArgs& a) {
                             const uint32_t r = wi * 4 + kk;
                             const uint32_t units = rset_units<ALIGNED>(g, r);
                             if (units) {
-                                q.rset[q.cnt++] = r;
-                                q.units += units;
+                                q.push(r, units);
                                 queued = true;
                             }
                         }
@@ -630,24 +639,35 @@ __device__ __forceinline__ void bfs_run(const BfsArgs& a) {
             const uint32_t W = (g.n + 31) / 32;
             const uint32_t tailMask = (g.n & 31) ? ((1u << (g.n & 31)) - 1) : 0xFFFFFFFFu;
             uint32_t longest = 0;
-            // The next word's visited/has-in words and row bounds are loaded
-            // while the current word is scanned (software pipeline).
-            uint32_t nvis = 0, nhin = 0xFFFFFFFFu, npb = 0, npe = 0;
-            auto prefetch = [&](uint32_t w) {
-                if (w < W) {
-                    nvis = __ldcg(&a.visited[w]);
-                    nhin = g.has_in ? __ldg(&g.has_in[w]) : 0xFFFFFFFFu;
-                    const uint32_t v = w * 32 + lane;
-                    npb = v < g.n ? __ldg(&g.csr_ptrs[v]) : 0u;
-                    npe = v < g.n ? __ldg(&g.csr_ptrs[v + 1]) : 0u;
-                }
-            };
-            prefetch(warp);
-            for (uint32_t wi = warp; wi < W; wi += nwarps) {
-                const uint32_t vis = nvis, hin = nhin, rb = npb, re = npe;
-                prefetch(wi + nwarps);
-                uint32_t unv = ~vis & (wi == W - 1 ? tailMask : 0xFFFFFFFFu) & hin;
-                if (unv == 0) continue;
+            // The warp's words are wi = warp + t * nwarps. Lane j loads the
+            // visited and has-in words of word t0 + j of each chunk of 32 in
+            // one go; the warp then walks only the words with unvisited
+            // vertices that have in-neighbours (a fully visited word costs no
+            // round trip of its own), with the next such word's row bounds
+            // loaded while the current one is scanned.
+            for (uint32_t t0 = 0; warp + t0 * nwarps < W; t0 += 32) {
+              const uint32_t wj = warp + (t0 + lane) * nwarps;
+              uint32_t visj = 0xFFFFFFFFu, unvj = 0;
+              if (wj < W) {
+                  visj = __ldcg(&a.visited[wj]);
+                  const uint32_t hj = g.has_in ? __ldg(&g.has_in[wj]) : 0xFFFFFFFFu;
+                  unvj = ~visj & hj & (wj == W - 1 ? tailMask : 0xFFFFFFFFu);
+              }
+              uint32_t todo = __ballot_sync(0xFFFFFFFFu, unvj != 0);
+              // row bounds of this lane's vertex in the next word with work
+              uint32_t nv = todo ? (warp + (t0 + __ffs(todo) - 1) * nwarps) * 32 + lane : g.n;
+              uint32_t npb = nv < g.n ? __ldg(&g.csr_ptrs[nv]) : 0u;
+              uint32_t npe = nv < g.n ? __ldg(&g.csr_ptrs[nv + 1]) : 0u;
+              while (todo) {
+                const uint32_t jj = __ffs(todo) - 1;
+                todo &= todo - 1;
+                const uint32_t wi = warp + (t0 + jj) * nwarps;
+                const uint32_t vis = __shfl_sync(0xFFFFFFFFu, visj, jj);
+                const uint32_t unv = __shfl_sync(0xFFFFFFFFu, unvj, jj);
+                const uint32_t rb = npb, re = npe;
+                nv = todo ? (warp + (t0 + __ffs(todo) - 1) * nwarps) * 32 + lane : g.n;
+                npb = nv < g.n ? __ldg(&g.csr_ptrs[nv]) : 0u;
+                npe = nv < g.n ? __ldg(&g.csr_ptrs[nv + 1]) : 0u;
                 bool found = false;
                 uint32_t parent = kUnreached;
                 const uint32_t u = wi * 32 + lane;
@@ -732,13 +752,13 @@ __device__ __forceinline__ void bfs_run(const BfsArgs& a) {
                     const uint32_t r = wi * 4 + lane;
                     const uint32_t units = rset_units<ALIGNED>(g, r);
                     if (units) {
-                        q.rset[q.cnt++] = r;
-                        q.units += units;
+                        q.push(r, units);
                         queued = true;
                     }
                 }
                 if (__ballot_sync(0xFFFFFFFFu, queued) && lane == 0) summary_set(a, fsum, wi);
                 flush_enqueue<ALIGNED>(a, q, kEnqueueCap - 1);
+              }
             }
             if (a.trace && lane == 0 && longest) atomicMax(&c->aux[6 + (level & 1)], (unsigned long long)longest);
             flush_enqueue<ALIGNED>(a, q);
@@ -799,8 +819,7 @@ __device__ __forceinline__ void bfs_run(const BfsArgs& a) {
                                 const uint32_t r = hu >> 3;
                                 const uint32_t units = rset_units<ALIGNED>(g, r);
                                 if (units) {
-                                    q.rset[q.cnt++] = r;
-                                    q.units += units;
+                                    q.push(r, units);
                                     summary_set(a, fsum, w);
                                 }
                             }
