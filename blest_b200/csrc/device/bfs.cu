@@ -468,9 +468,19 @@ __device__ __forceinline__ void bfs_run(const BfsArgs& a) {
             // while almost nothing is left unvisited; a grid after a pull
             // level has at most ~5x and is better off pushing. (Edges, not
             // tiles: full-padding tiles overstate a grid's push work.)
+            // Going to pull also needs the push work of this level (the
+            // queued rsets' tiles) to exceed 8x the pull's word visits: a
+            // grid's growing wavefront passes Beamer's test with ~3 tiles
+            // per word, and its pull, which scans every unvisited vertex,
+            // takes 2.5x as long as the push (grid 4096^2 levels 98/100:
+            // 250 us pulled, 95 us pushed), while RMAT's hub level (56
+            // tiles per word) and a uniform graph's big level (250) pull.
             const double mf = (double)(G1 - G2), mu = (double)(g.degree_total - G1);
             const bool growing = nf > nf_prev;
-            if (dir == BLEST_DIR_PUSH && mf * a.alpha > mu && growing) dir = BLEST_DIR_PULL;
+            const double push_tiles = (double)(U1 - U2) * (ALIGNED ? 32.0 : 1.0);
+            if (dir == BLEST_DIR_PUSH && mf * a.alpha > mu && growing &&
+                push_tiles > 8.0 * (double)((g.n + 31) / 32))
+                dir = BLEST_DIR_PULL;
             else if (dir == BLEST_DIR_PULL && (double)nf * a.beta < (double)g.n &&
                      mf < 8.0 * (double)((g.n + 31) / 32))
                 dir = BLEST_DIR_PUSH;
