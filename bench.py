@@ -290,12 +290,19 @@ def run_mbfs(args, rank, world):
     reached = (out != -1)
     mr = int(((reached.to(torch.int64) * deg).sum(1) // 2).sum().item())
     del reached
+    parity = None
     if rank == 0 and not args.skip_check:
+        # every source's levels against the oracle's OpenMP BFS
         import oracle as O
-        for i in (0, k - 1):
-            want = O.bfs_csc(n, csc.col_ptrs, csc.rows, int(sources[i]))
+        bad = 0
+        for i in range(k):
+            want, _ = O.bfs_omp(n, csc.col_ptrs, csc.rows, csr.col_ptrs, csr.rows, int(sources[i]), 0)
             if not np.array_equal(out[i].cpu().numpy().view(np.uint32), want):
-                raise SystemExit(f"MBFS levels differ from the oracle for source #{i}")
+                bad += 1
+                log(f"[parity] MBFS source #{i} differs from the oracle")
+        parity = {"sources_checked": k, "mismatches": bad, "against": "oracle bfs_omp (oracle/oracle.c), all sources"}
+        if bad:
+            raise SystemExit(f"MBFS levels differ from the oracle for {bad} of {k} sources")
     for _ in range(args.warmup):
         mbfs_once()
     barrier()
@@ -363,9 +370,11 @@ def run_mbfs(args, rank, world):
                 "d2h_bytes_per_step": 4 * k_e * n, "note": f"host output, {k_e} sources per step, host wall time"},
         "gpu_launches": args.steps,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "peak_source": peak_kind, "traffic": None,
+                     "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                     "traffic": profiled_traffic(args.workload),
                      "algorithmic_bytes_per_launch": out_bytes, "note": "output levels only (lower bound)"},
         "clocks": clocks.summary(),
+        "parity": parity,
     }
 
 
@@ -409,23 +418,21 @@ def _multi_worker_init():
 
 def _build_multi_graph(job):
     """One graph of the batch: generate, sample k sources (original ids),
-    Jaccard-reorder, build the BVSS, save both; returns the sources in
-    reordered ids."""
-    from blest_b200 import Bvss
+    Jaccard-reorder, save the CSC; returns the sources in reordered ids.
+    (Its BVSS is built on the device when the graph is uploaded.)"""
     i, n, ef, k, tag = job
     csc = rmat_n(n, ef, SEED + 1 + i)
     s = csc.sample_sources(k, SEED + i)
     inv = csc.reorder("jaccard", window=65536)
     csc.save_bin(f"{tag}/g{i}_csc.bin")
-    Bvss.build(csc).save_bin(f"{tag}/g{i}_bvss.bin")
     return i, np.asarray(inv[s], dtype=np.uint32)
 
 
 def prepare_multi(cache_dir: Path, rank: int, count: int = MULTI_GRAPHS, k: int = MULTI_SOURCES):
-    """The batch's graphs (Jaccard-reordered CSC + BVSS) and k sources each,
-    built by rank 0 into the cache and loaded by every rank."""
-    from blest_b200 import Bvss, Csc
-    tag = cache_dir / f"mbfs_multi{count}"
+    """The batch's graphs (Jaccard-reordered CSCs) and k sources each, built
+    by rank 0 into the cache and loaded by every rank."""
+    from blest_b200 import Csc
+    tag = cache_dir / f"mbfs_multi{count}_v2"
     done = tag / "ready"
     if rank == 0 and not done.exists():
         import multiprocessing as mp
@@ -447,10 +454,7 @@ def prepare_multi(cache_dir: Path, rank: int, count: int = MULTI_GRAPHS, k: int 
             if time.time() > deadline:
                 raise TimeoutError("graph cache not ready")
             time.sleep(1.0)
-    graphs = []
-    for i in range(count):
-        csc = Csc.load_bin(str(tag / f"g{i}_csc.bin"))
-        graphs.append((csc, Bvss.load_bin(str(tag / f"g{i}_bvss.bin"))))
+    graphs = [Csc.load_bin(str(tag / f"g{i}_csc.bin")) for i in range(count)]
     return graphs, np.load(str(tag / "sources.npy"))
 
 
@@ -469,10 +473,14 @@ def run_mbfs_multi(args, rank, world):
     blest_b200.init(dev)
     kind, gen, order, window, nsrc, desc = WORKLOADS[args.workload]
     t0 = time.time()
-    hosts, sources = prepare_multi(Path(args.cache), rank, MULTI_GRAPHS, nsrc)
+    cscs, sources = prepare_multi(Path(args.cache), rank, MULTI_GRAPHS, nsrc)
     t_prep = time.time() - t0
-    graphs = [Graph(b, c) for c, b in hosts]
-    ns = [c.n for c, _ in hosts]
+    # the BVSS of every graph is built on the device at upload
+    t1 = time.time()
+    graphs = [Graph.from_csc(c) for c in cscs]
+    t_upload = time.time() - t1
+    from blest_b200 import Bvss
+    ns = [c.n for c in cscs]
     k = sources.shape[1]
     total = sum(ns) * k
     out = torch.empty(total, dtype=torch.int32, device="cuda")
@@ -506,7 +514,8 @@ def run_mbfs_multi(args, rank, world):
     plan.run()
     # reached edges and algorithmic bytes per step, from the levels
     mr, s_r, v_r, n_r = 0, 0, 0, 0
-    for (csc, bvss), lv in zip(hosts, views):
+    for csc, lv in zip(cscs, views):
+        bvss = Bvss.build_device(csc)  # for the algorithmic-byte count only
         deg = torch.from_numpy(np.diff(csc.col_ptrs.astype(np.int64))).cuda()
         reached = lv != -1
         mr += int(((reached.to(torch.int64) * deg).sum(1) // 2).sum().item())
@@ -518,15 +527,25 @@ def run_mbfs_multi(args, rank, world):
         v_r += int((rp[rsets + 1].astype(np.int64) - rp[rsets]).sum())
         s_r += int((ssp[rp[rsets + 1]].astype(np.int64) - ssp[rp[rsets]].astype(np.int64)).sum())
     algo = 5 * s_r + 12 * v_r + 4 * n_r
+    parity = None
     if rank == 0 and not args.skip_check:
+        # every (graph, source) pair against the oracle
         import oracle as O
-        big = int(np.argmax(ns))
-        for i in (0, 1, big, len(graphs) - 1):
-            csc = hosts[i][0]
-            for j in (0, k - 1):
+        bad = 0
+        host_levels = out.cpu().numpy().view(np.uint32)
+        o = 0
+        for i, csc in enumerate(cscs):
+            lv = host_levels[o:o + k * csc.n].reshape(k, csc.n)
+            o += k * csc.n
+            for j in range(k):
                 want = O.bfs_csc(csc.n, csc.col_ptrs, csc.rows, int(sources[i][j]))
-                if not np.array_equal(views[i][j].cpu().numpy().view(np.uint32), want):
-                    raise SystemExit(f"multi-graph MBFS levels differ from the oracle (graph {i}, source {j})")
+                if not np.array_equal(lv[j], want):
+                    bad += 1
+                    log(f"[parity] multi-graph MBFS graph {i} source {j} differs from the oracle")
+        parity = {"sources_checked": int(k * len(cscs)), "mismatches": bad,
+                  "against": "oracle bfs_csc (oracle/oracle.c), every (graph, source) pair"}
+        if bad:
+            raise SystemExit(f"multi-graph MBFS levels differ from the oracle for {bad} pairs")
     stream = torch.cuda.current_stream()
     for _ in range(args.warmup):
         plan.run()
@@ -605,7 +624,7 @@ def run_mbfs_multi(args, rank, world):
         "config": {"workload": args.workload, "description": desc, "graphs": len(graphs),
                    "sources_per_graph": k, "vertices_total": int(sum(ns)),
                    "n_min": int(min(ns)), "n_median": int(np.median(ns)), "n_max": int(max(ns)),
-                   "nnz_total": int(sum(c.nnz for c, _ in hosts)), "joined_n": int(info.n),
+                   "nnz_total": int(sum(c.nnz for c in cscs)), "joined_n": int(info.n),
                    "captured_cuda_graph": bool(info.captured), "grid_blocks": int(info.grid_blocks),
                    "autotuned": tuned, "autotune_table_ms": [[round(t * 1e3, 3), p] for t, p in table],
                    "reached_edges_per_step": mr,
@@ -615,14 +634,17 @@ def run_mbfs_multi(args, rank, world):
                    "speedup_vs_per_graph": round(value / world / per_graph, 2),
                    "host_wall_ms_per_step": round(wall * 1e3 / args.steps, 4),
                    "prep_seconds": round(t_prep, 1),
+                   "upload_with_device_bvss_seconds": round(t_upload, 2),
                    "l2": "outputs larger than L2, no flush"},
         "e2e": {"value": round(e2e, 3), "unit": "GTEPS", "h2d_bytes_per_step": 4 * int(sources.size),
                 "d2h_bytes_per_step": 4 * total},
         "gpu_launches": args.steps,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "peak_source": peak_kind, "traffic": None,
+                     "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                     "traffic": profiled_traffic(args.workload),
                      "algorithmic_bytes_per_launch": algo, "avg_launch_ms": round(kern_s * 1e3, 4)},
         "clocks": clocks.summary(),
+        "parity": parity,
     }
 
 
@@ -965,6 +987,18 @@ def run_b200(args, rank, world):
         dist.all_reduce(e2e_ms_t, op=dist.ReduceOp.MAX)
     e2e_ms = float(e2e_ms_t.item())
     e2e = edges_per_step * args.steps * world / (e2e_ms * 1e-3) / 1e9
+    # the copy bound of e2e: one level array per BFS at the measured
+    # device-to-host bandwidth into pinned memory
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    bufs[0].copy_(out, non_blocking=True)
+    c0.record(stream)
+    with torch.cuda.stream(stream):
+        for _ in range(16):
+            bufs[0].copy_(out, non_blocking=True)
+    c1.record(stream)
+    stream.synchronize()
+    d2h_gbs = 16 * 4.0 * n / (c0.elapsed_time(c1) * 1e-3) / 1e9
+    copy_bound = edges_per_step / (len(sources) * 4.0 * n / (d2h_gbs * 1e9)) / 1e9
     if check:
         # the last pipelined result must still equal the oracle's
         last = sources[-1]
@@ -1009,7 +1043,9 @@ def run_b200(args, rank, world):
                                            "convention (BFS/BVSSBFSKernel.cuh:1469,1545-1548)"},
         "e2e": {"value": round(e2e, 3), "unit": "GTEPS", "h2d_bytes_per_step": 4 * int(len(sources)),
                 "d2h_bytes_per_step": 4 * n * int(len(sources)),
-                "note": "blest_bfs_ws with pinned host output, copy of BFS i overlapped with BFS i + 1"},
+                "note": "blest_bfs_ws with pinned host output, copy of BFS i overlapped with BFS i + 1",
+                "d2h_gbs_measured": round(d2h_gbs, 2), "copy_bound_gteps": round(copy_bound, 3),
+                "frac_of_copy_bound": round(e2e / world / copy_bound, 3)},
         "gpu_launches": int(len(sources)) * args.steps,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_source": peak_kind,
@@ -1107,9 +1143,11 @@ def run_cc(args, rank, world):
                 "d2h_bytes_per_step": 4 * n},
         "gpu_launches": 4 * args.steps,  # init, queue seed, persistent propagation, component count
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "peak_source": peak_kind, "traffic": None,
+                     "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                     "traffic": profiled_traffic(args.workload),
                      "algorithmic_bytes_per_launch": algo, "avg_launch_ms": round(kern_s * 1e3, 4)},
         "clocks": clocks.summary(),
+        "parity": parity,
     }
     if parity:
         result["parity"] = parity
