@@ -1021,8 +1021,9 @@ def run_b200(args, rank, world):
                 f"(push {st.push_levels}, pull {st.pull_levels})")
             for i in range(cnt.value - 1):
                 r, nx = recs[i], recs[i + 1]
+                sweep = f" (sweep {(nx.start_ns - r.sweep_ns) / 1e3:.1f} us)" if r.sweep_ns else ""
                 log(f"[trace]   L{r.level:<4d} {'push' if r.direction == 1 else 'pull'} frontier {r.frontier:>9d} "
-                    f"units {r.work_units:>10d} {(nx.start_ns - r.start_ns) / 1e3:9.1f} us")
+                    f"units {r.work_units:>10d} {(nx.start_ns - r.start_ns) / 1e3:9.1f} us{sweep}")
     peak, peak_kind = measured_peak()
     avg_bytes = float(np.mean(algo))
     avg_launch_s = float(np.mean(bfs_ms)) * 1e-3

@@ -85,7 +85,7 @@ class BfsParams(C.Structure):
 
 class LevelTrace(C.Structure):
     _fields_ = [("start_ns", u64), ("level", u32), ("direction", u32), ("frontier", u64), ("work_units", u64),
-                ("longest_scan", u64)]
+                ("longest_scan", u64), ("sweep_ns", u64)]
 
 
 class BfsStats(C.Structure):

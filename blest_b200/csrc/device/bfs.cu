@@ -450,6 +450,7 @@ __device__ __forceinline__ void bfs_run(const BfsArgs& a) {
                     t.direction = 0;
                     t.frontier = 0;
                     t.work_units = 0;
+                    t.sweep_ns = 0;
                 }
             }
             break;
@@ -493,6 +494,7 @@ __device__ __forceinline__ void bfs_run(const BfsArgs& a) {
             t.direction = (uint32_t)dir;
             t.frontier = nf;
             t.work_units = (uint64_t)(U1 - U2);
+            t.sweep_ns = 0;
             // longest warp-finished scan of the previous level; its slot is
             // then free for the next level
             if (level >= 2) a.trace[level - 2].longest_scan = ld_relaxed64(&c->aux[6 + ((level - 1) & 1)]);
@@ -589,6 +591,7 @@ __device__ __forceinline__ void bfs_run(const BfsArgs& a) {
             }
             if (lazy) {
                 if (!grid_barrier(c)) return;
+                if (a.trace && tid == 0 && level <= BLEST_TRACE_CAPACITY) a.trace[level - 1].sweep_ns = global_ns();
                 // Sweep: lane j of a warp takes word base + j (candidates,
                 // visited, rsets to queue); then the warp walks those 32
                 // words with one lane per vertex for coalesced level writes

@@ -406,6 +406,7 @@ __global__ void __launch_bounds__(512, 2) mbfs_persistent_kernel(MbfsArgs a) {
                 t.frontier = nf;
                 t.work_units = ld_relaxed64(&c->aux[slot]) & kQUnitMask;
                 t.longest_scan = grp;
+                t.sweep_ns = 0;
             }
             if (nf == 0) break;
             if (level > n + 1) {

@@ -263,6 +263,7 @@ typedef struct blest_level_trace {
     uint64_t frontier;        /* vertices discovered at the previous level */
     uint64_t work_units;      /* tiles (32-tile chunks with the MMA test) of the queued rsets */
     uint64_t longest_scan;    /* pull: longest in-neighbour list finished by a whole warp */
+    uint64_t sweep_ns;        /* lazy push level: %globaltimer when its word sweep started (0 otherwise) */
 } blest_level_trace;
 #define BLEST_TRACE_CAPACITY 4096
 
