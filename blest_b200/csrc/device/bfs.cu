@@ -638,26 +638,32 @@ __device__ __forceinline__ void bfs_run(const BfsArgs& a) {
                 }
             }
         } else {
-            // Bottom-up: each warp owns whole 32-vertex words. Each lane scans
-            // its unvisited vertex's in-neighbours four at a time
+            // Bottom-up. A warp owns the words wi = warp + t * nwarps and
+            // takes them 32 at a time: lane j loads word j's visited and
+            // has-in words, and the unvisited vertices with in-neighbours of
+            // all 32 words are compacted into one list (a warp scan of their
+            // counts) that the lanes take 32 at a time, so no lane idles on a
+            // visited vertex (a uniform graph's first pull level has ~12 per
+            // word). Each lane scans its vertex's in-neighbours four at a time
             // (independent loads) for at most kPullLaneScan neighbours; the
             // warp then finishes the longer lists together, one vertex at a
             // time, 32 neighbours per coalesced step, stopping at the first
-            // frontier neighbour. A neighbour's frontier word is read from L2
-            // only when the level's summary (staged in shared memory) says
-            // it is non-empty; vertices without in-neighbours are skipped.
+            // frontier neighbour; very long lists go to the heavy queue. The
+            // next round's row bounds are loaded while the current round is
+            // scanned. Found vertices set their bit in the warp's word slots
+            // in shared memory; after the chunk, lane j writes word j's
+            // visited/frontier words (the warp owns them), its levels (one
+            // 128-byte segment) and queues its rsets. A neighbour's frontier
+            // word is read from L2 only when the level's summary (staged in
+            // shared memory) says it is non-empty.
             const uint32_t* sprev = summary_buf(a, level - 1);
             for (uint32_t i = threadIdx.x; i < a.sum_words; i += blockDim.x) s_sum[i] = __ldcg(&sprev[i]);
             __syncthreads();
             const uint32_t W = (g.n + 31) / 32;
             const uint32_t tailMask = (g.n & 31) ? ((1u << (g.n & 31)) - 1) : 0xFFFFFFFFu;
             uint32_t longest = 0;
-            // The warp's words are wi = warp + t * nwarps. Lane j loads the
-            // visited and has-in words of word t0 + j of each chunk of 32 in
-            // one go; the warp then walks only the words with unvisited
-            // vertices that have in-neighbours (a fully visited word costs no
-            // round trip of its own), with the next such word's row bounds
-            // loaded while the current one is scanned.
+            __shared__ uint32_t s_found[512];  // 32 word slots per warp of the block
+            uint32_t* found_slots = s_found + (threadIdx.x & ~31u);
             for (uint32_t t0 = 0; warp + t0 * nwarps < W; t0 += 32) {
               const uint32_t wj = warp + (t0 + lane) * nwarps;
               uint32_t visj = 0xFFFFFFFFu, unvj = 0;
@@ -666,26 +672,48 @@ __device__ __forceinline__ void bfs_run(const BfsArgs& a) {
                   const uint32_t hj = g.has_in ? __ldg(&g.has_in[wj]) : 0xFFFFFFFFu;
                   unvj = ~visj & hj & (wj == W - 1 ? tailMask : 0xFFFFFFFFu);
               }
-              uint32_t todo = __ballot_sync(0xFFFFFFFFu, unvj != 0);
-              // row bounds of this lane's vertex in the next word with work
-              uint32_t nv = todo ? (warp + (t0 + __ffs(todo) - 1) * nwarps) * 32 + lane : g.n;
-              uint32_t npb = nv < g.n ? __ldg(&g.csr_ptrs[nv]) : 0u;
-              uint32_t npe = nv < g.n ? __ldg(&g.csr_ptrs[nv + 1]) : 0u;
-              while (todo) {
-                const uint32_t jj = __ffs(todo) - 1;
-                todo &= todo - 1;
-                const uint32_t wi = warp + (t0 + jj) * nwarps;
-                const uint32_t vis = __shfl_sync(0xFFFFFFFFu, visj, jj);
-                const uint32_t unv = __shfl_sync(0xFFFFFFFFu, unvj, jj);
-                const uint32_t rb = npb, re = npe;
-                nv = todo ? (warp + (t0 + __ffs(todo) - 1) * nwarps) * 32 + lane : g.n;
-                npb = nv < g.n ? __ldg(&g.csr_ptrs[nv]) : 0u;
-                npe = nv < g.n ? __ldg(&g.csr_ptrs[nv + 1]) : 0u;
+              // exclusive offsets of the words' items in the chunk's list
+              const uint32_t cj = __popc(unvj);
+              uint32_t incl = cj;
+#pragma unroll
+              for (uint32_t d = 1; d < 32; d <<= 1) {
+                  const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+                  if (lane >= d) incl += o;
+              }
+              const uint32_t offj = incl - cj;
+              const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+              if (total == 0) continue;
+              found_slots[lane] = 0u;
+              __syncwarp();
+              // item idx -> (word slot, vertex); warp-uniform call
+              auto item = [&](uint32_t idx, uint32_t& slot, uint32_t& vtx) {
+                  uint32_t lo = 0;
+#pragma unroll
+                  for (uint32_t st = 16; st > 0; st >>= 1) {
+                      const uint32_t cand = lo + st;
+                      const uint32_t o = __shfl_sync(0xFFFFFFFFu, offj, cand & 31);
+                      if (cand < 32 && o <= idx) lo = cand;
+                  }
+                  const uint32_t o = __shfl_sync(0xFFFFFFFFu, offj, lo);
+                  const uint32_t um = __shfl_sync(0xFFFFFFFFu, unvj, lo);
+                  slot = lo;
+                  vtx = idx < total ? (warp + (t0 + lo) * nwarps) * 32 + __fns(um, 0, (int)(idx - o + 1)) : kUnreached;
+              };
+              uint32_t nslot, nvtx;
+              item(lane, nslot, nvtx);
+              uint32_t npb = nvtx < g.n ? __ldg(&g.csr_ptrs[nvtx]) : 0u;
+              uint32_t npe = nvtx < g.n ? __ldg(&g.csr_ptrs[nvtx + 1]) : 0u;
+              for (uint32_t base = 0; base < total; base += 32) {
+                const uint32_t myslot = nslot, u = nvtx, rb = npb, re = npe;
+                if (base + 32 < total) {
+                    item(base + 32 + lane, nslot, nvtx);
+                    npb = nvtx < g.n ? __ldg(&g.csr_ptrs[nvtx]) : 0u;
+                    npe = nvtx < g.n ? __ldg(&g.csr_ptrs[nvtx + 1]) : 0u;
+                }
                 bool found = false;
                 uint32_t parent = kUnreached;
-                const uint32_t u = wi * 32 + lane;
                 uint32_t pb = 0, pe = 0, p = 0;
-                if ((unv >> lane) & 1u) {
+                if (u < g.n) {
                     pb = rb;
                     pe = re;
                     p = pb;
@@ -713,11 +741,11 @@ __device__ __forceinline__ void bfs_run(const BfsArgs& a) {
                     const bool heavy = !found && p < pe && pe - p > a.heavy_min;
                     if (heavy) {
                         const uint32_t chunks = (pe - p + kHeavyChunk - 1) / kHeavyChunk;
-                        const uint64_t slot = atomicAdd(&c->lvl[level % 3][3],
-                                                        (unsigned long long)((1ull << kQShift) | chunks));
-                        const uint32_t idx = (uint32_t)(slot >> kQShift);
+                        const uint64_t hs = atomicAdd(&c->lvl[level % 3][3],
+                                                      (unsigned long long)((1ull << kQShift) | chunks));
+                        const uint32_t idx = (uint32_t)(hs >> kQShift);
                         if (idx < a.heavy_cap) {
-                            a.heavy[idx] = make_uint4(u, p, pe, (uint32_t)(slot & kQUnitMask));
+                            a.heavy[idx] = make_uint4(u, p, pe, (uint32_t)(hs & kQUnitMask));
                             p = pe;  // handed over
                         } else {
                             set_error(c, BLEST_ERR_DEVICE_INDEX);  // capacity is sized so this cannot happen
@@ -733,8 +761,8 @@ __device__ __forceinline__ void bfs_run(const BfsArgs& a) {
                     const uint32_t q1 = __shfl_sync(0xFFFFFFFFu, pe, ln);
                     longest = max(longest, q1 - q0);
                     uint32_t hitv = kUnreached;
-                    for (uint32_t base = q0; base < q1; base += 32) {
-                        const uint32_t idx = base + lane;
+                    for (uint32_t qb = q0; qb < q1; qb += 32) {
+                        const uint32_t idx = qb + lane;
                         const uint32_t v = idx < q1 ? __ldg(&g.csr_ids[idx]) : kUnreached;
                         const bool f = v != kUnreached && in_frontier(v);
                         const uint32_t hb = __ballot_sync(0xFFFFFFFFu, f);
@@ -748,30 +776,35 @@ __device__ __forceinline__ void bfs_run(const BfsArgs& a) {
                         parent = hitv;
                     }
                 }
-                const uint32_t nb = __ballot_sync(0xFFFFFFFFu, found);
-                if (nb == 0) continue;
-                if (lane == 0) {
-                    a.visited[wi] = vis | nb;
-                    fcur[wi] = nb;
-                }
                 if (found) {
-                    a.levels[u] = level;
+                    atomicOr(&found_slots[myslot], 1u << (u & 31));
                     if (PARENTS) a.parents[u] = parent;
                     ++disc;
                     deg += pe - pb;
                 }
-                bool queued = false;
-                if (lane < 4 && ((nb >> (8 * lane)) & 0xFFu)) {
-                    const uint32_t r = wi * 4 + lane;
-                    const uint32_t units = rset_units<ALIGNED>(g, r);
-                    if (units) {
-                        q.push(r, units);
-                        queued = true;
-                    }
-                }
-                if (__ballot_sync(0xFFFFFFFFu, queued) && lane == 0) summary_set(a, fsum, wi);
-                flush_enqueue<ALIGNED>(a, q, kEnqueueCap - 1);
               }
+              __syncwarp();
+              // write back the chunk's words (lane j: word j)
+              const uint32_t nb = found_slots[lane];
+              bool queued = false;
+              if (nb) {
+                  a.visited[wj] = visj | nb;
+                  fcur[wj] = nb;
+                  for (uint32_t m = nb; m; m &= m - 1) a.levels[wj * 32 + __ffs(m) - 1] = level;
+#pragma unroll
+                  for (uint32_t k = 0; k < 4; ++k) {
+                      if ((nb >> (8 * k)) & 0xFFu) {
+                          const uint32_t r = wj * 4 + k;
+                          const uint32_t units = rset_units<ALIGNED>(g, r);
+                          if (units) {
+                              q.push(r, units);
+                              queued = true;
+                          }
+                      }
+                  }
+                  if (queued) summary_set(a, fsum, wj);
+              }
+              flush_enqueue<ALIGNED>(a, q, kEnqueueCap - 4);
             }
             if (a.trace && lane == 0 && longest) atomicMax(&c->aux[6 + (level & 1)], (unsigned long long)longest);
             flush_enqueue<ALIGNED>(a, q);
