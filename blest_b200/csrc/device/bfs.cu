@@ -623,16 +623,31 @@ __device__ __forceinline__ void bfs_run(const BfsArgs& a) {
                     }
                     if (queued) summary_set(a, fsum, wi);
                     flush_enqueue<ALIGNED>(a, q, kEnqueueCap - 4);
-                    uint32_t words = __ballot_sync(0xFFFFFFFFu, nw != 0);
-                    while (words) {
-                        const uint32_t j = __ffs(words) - 1;
-                        words &= words - 1;
-                        const uint32_t bits = __shfl_sync(0xFFFFFFFFu, nw, j);
-                        if ((bits >> lane) & 1u) {
-                            const uint32_t v = (base + j) * 32 + lane;
-                            a.levels[v] = level;
-                            ++disc;
-                            deg += __ldg(&g.csr_ptrs[v + 1]) - __ldg(&g.csr_ptrs[v]);
+                    // 8 words at a time: all their degree loads are issued
+                    // before any is added (the sum would otherwise hold each
+                    // load's latency in turn)
+                    const uint32_t words = __ballot_sync(0xFFFFFFFFu, nw != 0);
+                    for (uint32_t j0 = 0; j0 < 32; j0 += 8) {
+                        if (!((words >> j0) & 0xFFu)) continue;
+                        uint32_t d0[8], d1[8], vb = 0;
+#pragma unroll
+                        for (uint32_t k = 0; k < 8; ++k) {
+                            const uint32_t bits = __shfl_sync(0xFFFFFFFFu, nw, j0 + k);
+                            const uint32_t v = (base + j0 + k) * 32 + lane;
+                            d0[k] = d1[k] = 0u;
+                            if ((bits >> lane) & 1u) {
+                                vb |= 1u << k;
+                                d0[k] = __ldg(&g.csr_ptrs[v]);
+                                d1[k] = __ldg(&g.csr_ptrs[v + 1]);
+                            }
+                        }
+#pragma unroll
+                        for (uint32_t k = 0; k < 8; ++k) {
+                            if ((vb >> k) & 1u) {
+                                a.levels[(base + j0 + k) * 32 + lane] = level;
+                                ++disc;
+                                deg += d1[k] - d0[k];
+                            }
                         }
                     }
                 }
