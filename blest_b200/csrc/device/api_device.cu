@@ -268,6 +268,9 @@ void finish_one(blest_workspace* ws, blest_bfs_stats* st) {
         // slot; either way the slot's last copy is then done
         BLEST_CUDA(cudaEventSynchronize(ws->ev_copy[slot]));
         ws->slot_busy[slot] = false;
+    } else if (slot < 0 && seq + 1 == ws->issued) {
+        // the last call issued: the stream's completion is this call's
+        BLEST_CUDA(cudaStreamSynchronize(ws->stream));
     } else if (slot < 0) {
         // Wait for this call's record only (later calls keep running): its
         // kernel writes seq last, after a system-scope fence. If the stream
