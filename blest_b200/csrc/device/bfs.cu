@@ -84,7 +84,7 @@ __device__ __forceinline__ void summary_set(const BfsArgs& a, uint32_t* sum, uin
 // and how many of them it has in flight at once (a warp waits for its
 // slowest lane, so fewer, wider rounds finish sooner).
 constexpr uint32_t kPullLaneScan = 32;
-constexpr uint32_t kPullUnroll = 4;
+constexpr uint32_t kPullUnroll = 8;
 // Neighbours per piece of a heavy (very long) in-neighbour list.
 constexpr uint32_t kHeavyChunk = 256;
 
@@ -792,10 +792,19 @@ __device__ __forceinline__ void bfs_run(const BfsArgs& a) {
                     }
                 }
                 if (found) {
-                    atomicOr(&found_slots[myslot], 1u << (u & 31));
                     if (PARENTS) a.parents[u] = parent;
                     ++disc;
                     deg += pe - pb;
+                }
+                // this round's found bits, merged per word slot by a warp
+                // reduction: one store per distinct slot (lanes of one word
+                // would otherwise collide on the same shared-memory word)
+                for (uint32_t pending = __ballot_sync(0xFFFFFFFFu, found); pending;) {
+                    const uint32_t slot = __shfl_sync(0xFFFFFFFFu, myslot, __ffs(pending) - 1);
+                    const bool mine = found && myslot == slot;
+                    const uint32_t bits = __reduce_or_sync(0xFFFFFFFFu, mine ? 1u << (u & 31) : 0u);
+                    if (lane == 0) found_slots[slot] |= bits;
+                    pending &= ~__ballot_sync(0xFFFFFFFFu, mine);
                 }
               }
               __syncwarp();
