@@ -246,46 +246,81 @@ __device__ __forceinline__ void discover4(const BfsArgs& a, uint32_t* fcur, uint
 }
 
 // One push step's operands: the tile of this lane (row ids, mask word),
-// the frontier byte of its rset, and the queue owner of the next step.
+// the frontier byte of its rset and the rset.
 struct StepLoad {
     uint4 rows;
     uint32_t mask;
     uint32_t fb;
     uint32_t r;
-    uint32_t next_owner;
 };
 
-// Resolve the queue entry of each lane's position in the step starting at
-// unit `base` (entries owner..owner+31 can cover it) and issue its loads.
-template <bool ALIGNED>
-__device__ __forceinline__ StepLoad load_step(const BfsArgs& a, const uint32_t* fprev, uint32_t owner, uint32_t E1,
-                                              uint32_t U1, uint32_t base, RunCounters* c) {
+// A warp's cached view of 32 consecutive queue entries [w0, w0 + 32): lane e
+// holds entry w0 + e's first unit, rset, tile range and frontier byte, and
+// `end` is the unit where the window's coverage ends. A push step then
+// finds its entries by shuffles alone; the window is reloaded only when a
+// step runs past `end` (an rset of 64 tiles, as on a uniform graph, keeps
+// one window for 64 steps), instead of two dependent load rounds per step.
+struct QueueWindow {
+    uint32_t w0, end;
+    uint32_t eoff, ers, et0, et1, efb;
+};
+
+__device__ __forceinline__ void window_load(const BfsArgs& a, const uint32_t* fprev, QueueWindow& W, uint32_t w0,
+                                            uint32_t E1, uint32_t U1) {
     const uint32_t lane = threadIdx.x & 31;
-    const uint32_t ei = owner + lane;
+    const uint32_t ei = w0 + lane;
     const bool in = ei < E1;
-    const uint32_t eoff = in ? __ldcg(&a.q_off[ei]) : 0xFFFFFFFFu;
-    const uint32_t ers = in ? __ldcg(&a.q_rset[ei]) : 0u;
+    W.w0 = w0;
+    W.eoff = in ? __ldcg(&a.q_off[ei]) : 0xFFFFFFFFu;
+    W.ers = in ? __ldcg(&a.q_rset[ei]) : 0u;
+    W.end = w0 + 32 < E1 ? __ldcg(&a.q_off[w0 + 32]) : U1;
+    W.et0 = in ? __ldg(&a.g.rset_tile[W.ers]) : 0u;
+    W.et1 = in ? __ldg(&a.g.rset_tile[W.ers + 1]) : 0u;
+    W.efb = in ? (__ldcg(&fprev[W.ers >> 2]) >> (8 * (W.ers & 3))) & 0xFFu : 0u;
+}
+
+// Queue entries e in [lo, hi) with q_off sorted: the largest with
+// q_off[e] <= pos.
+__device__ __forceinline__ uint32_t find_owner(const uint32_t* q_off, uint32_t lo, uint32_t hi, uint32_t pos);
+
+// Make W cover the step of `span` units starting at `base` (< U1);
+// warp-uniform. After a reload from the entry holding `base`, the window
+// covers at least 32 units past it (every queued entry has a unit).
+__device__ __forceinline__ void window_cover(const BfsArgs& a, const uint32_t* fprev, QueueWindow& W, uint32_t base,
+                                             uint32_t span, uint32_t E1, uint32_t U1) {
+    if (min(base + span, U1) - 1 < W.end) return;
+    const uint32_t w0 = base < W.end ? W.w0 + __popc(__ballot_sync(0xFFFFFFFFu, W.eoff <= base)) - 1
+                                     : find_owner(a.q_off, W.w0 + 32, E1, base);
+    window_load(a, fprev, W, w0, E1, U1);
+}
+
+// The step starting at unit `base` from the covering window: each lane's
+// entry by shuffles, then its tile's loads.
+template <bool ALIGNED>
+__device__ __forceinline__ StepLoad load_step(const BfsArgs& a, const QueueWindow& W, uint32_t U1, uint32_t base,
+                                              RunCounters* c) {
+    const uint32_t lane = threadIdx.x & 31;
     uint32_t pos, my;
     if (ALIGNED) {
         pos = base;
-        my = __popc(__ballot_sync(0xFFFFFFFFu, eoff <= pos)) - 1;
+        my = __popc(__ballot_sync(0xFFFFFFFFu, W.eoff <= pos)) - 1;
     } else {
         pos = base + lane;
         uint32_t lo = 0;
 #pragma unroll
         for (uint32_t st = 16; st > 0; st >>= 1) {
             const uint32_t cand = lo + st;
-            const uint32_t b = __shfl_sync(0xFFFFFFFFu, eoff, cand & 31);
+            const uint32_t b = __shfl_sync(0xFFFFFFFFu, W.eoff, cand & 31);
             if (cand < 32 && b <= pos) lo = cand;
         }
         my = lo;
     }
     StepLoad L;
-    L.r = __shfl_sync(0xFFFFFFFFu, ers, my);
-    const uint32_t off = __shfl_sync(0xFFFFFFFFu, eoff, my);
-    L.next_owner = owner + __shfl_sync(0xFFFFFFFFu, my, 31);
-    const uint32_t t0 = __ldg(&a.g.rset_tile[L.r]);
-    const uint32_t t1 = __ldg(&a.g.rset_tile[L.r + 1]);
+    L.r = __shfl_sync(0xFFFFFFFFu, W.ers, my);
+    const uint32_t off = __shfl_sync(0xFFFFFFFFu, W.eoff, my);
+    const uint32_t t0 = __shfl_sync(0xFFFFFFFFu, W.et0, my);
+    const uint32_t t1 = __shfl_sync(0xFFFFFFFFu, W.et1, my);
+    L.fb = __shfl_sync(0xFFFFFFFFu, W.efb, my);
     uint32_t tile;
     bool valid;
     if (ALIGNED) {
@@ -300,7 +335,6 @@ __device__ __forceinline__ StepLoad load_step(const BfsArgs& a, const uint32_t* 
         set_error(c, BLEST_ERR_DEVICE_INDEX);
         valid = false;
     }
-    L.fb = (__ldcg(&fprev[L.r >> 2]) >> (8 * (L.r & 3))) & 0xFFu;
     L.rows = make_uint4(0, 0, 0, 0);
     L.mask = 0;
     if (valid) {
@@ -545,17 +579,24 @@ __device__ __forceinline__ void bfs_run(const BfsArgs& a) {
                 for (uint32_t kk = 0; kk < 4; ++kk) h |= (((t.mask >> (8 * kk)) & t.fb & 0xFFu) ? 1u : 0u) << kk;
                 return h;
             };
+            QueueWindow qw;
+            if (s < send) {
+                window_load(a, fprev, qw, find_owner(a.q_off, E2, E1, U2 + s * per), E1, U1);
+                window_cover(a, fprev, qw, U2 + s * per, per, E1, U1);
+            }
             if (s < send && lazy) {
                 // Lazy levels claim nothing and queue nothing, which leaves
-                // registers to software-pipeline the steps: the loads of
-                // step s + 1 (queue entry, tile range, tile) are in flight
-                // while step s's hit rows are checked and ORed.
-                StepLoad cur = load_step<ALIGNED>(a, fprev, find_owner(a.q_off, E2, E1, U2 + s * per), E1, U1,
-                                                  U2 + s * per, c);
+                // registers to software-pipeline the steps: the tile loads
+                // of step s + 1 are in flight while step s's hit rows are
+                // checked and ORed.
+                StepLoad cur = load_step<ALIGNED>(a, qw, U1, U2 + s * per, c);
                 for (; s < send; ++s) {
                     const bool more = s + 1 < send;  // warp-uniform
                     StepLoad nxt;
-                    if (more) nxt = load_step<ALIGNED>(a, fprev, cur.next_owner, E1, U1, U2 + (s + 1) * per, c);
+                    if (more) {
+                        window_cover(a, fprev, qw, U2 + (s + 1) * per, per, E1, U1);
+                        nxt = load_step<ALIGNED>(a, qw, U1, U2 + (s + 1) * per, c);
+                    }
                     const uint32_t hits = tile_hits(cur);
                     if (hits) {
                         const uint32_t rowk[4] = {cur.rows.x, cur.rows.y, cur.rows.z, cur.rows.w};
@@ -576,10 +617,9 @@ __device__ __forceinline__ void bfs_run(const BfsArgs& a) {
                     if (more) cur = nxt;
                 }
             } else if (s < send) {
-                uint32_t owner = find_owner(a.q_off, E2, E1, U2 + s * per);
                 for (; s < send; ++s) {
-                    const StepLoad cur = load_step<ALIGNED>(a, fprev, owner, E1, U1, U2 + s * per, c);
-                    owner = cur.next_owner;
+                    window_cover(a, fprev, qw, U2 + s * per, per, E1, U1);
+                    const StepLoad cur = load_step<ALIGNED>(a, qw, U1, U2 + s * per, c);
                     const uint32_t hits = tile_hits(cur);
                     if (hits) {
                         const uint32_t rowk[4] = {cur.rows.x, cur.rows.y, cur.rows.z, cur.rows.w};
