@@ -84,7 +84,7 @@ __device__ __forceinline__ void summary_set(const BfsArgs& a, uint32_t* sum, uin
 // and how many of them it has in flight at once (a warp waits for its
 // slowest lane, so fewer, wider rounds finish sooner).
 constexpr uint32_t kPullLaneScan = 32;
-constexpr uint32_t kPullUnroll = 8;
+constexpr uint32_t kPullUnroll = 4;
 // Neighbours per piece of a heavy (very long) in-neighbour list.
 constexpr uint32_t kHeavyChunk = 256;
 
