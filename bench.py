@@ -1163,31 +1163,50 @@ def run_cc(args, rank, world):
     return result
 
 
-def prepare_reference(workload: str):
+def prepare_reference(workload: str, cache_dir: Path):
     """The workload's graph built by the REFERENCE's own host code through
     oracle/_ref (never libblest_b200.so): the oracle generator's CSC (the
     same bytes as the library's generator), the reference's CSC object and
     classification, its ordering (Jaccard window or RCM), its BVSS builder
     with FULL_PADDING = !social (Benchmark.cuh:113-114, 187-194), and the
-    seeded sources mapped to the new ids as Benchmark.cuh:80 does."""
+    seeded sources mapped to the new ids as Benchmark.cuh:80 does. Like the
+    reference's own driver, the reordered CSC is cached with its
+    CSC::saveToBinary (and read back with CSC::constructFromBinary), so the
+    BFS and CC workloads of one graph reorder it once."""
     import oracle as O
     kind, gen, order, window, nsrc, _ = WORKLOADS[workload]
+    cache_dir.mkdir(parents=True, exist_ok=True)
+    tag = cache_dir / f"reference_{'_'.join(map(str, gen))}_{order}_{window}"
+    counts = sorted({w[4] for w in WORKLOADS.values() if w[1:4] == (gen, order, window) and w[4]})
     t0 = time.time()
-    n, cp, rw = generate_oracle(gen)
-    src = O.sample_sources(n, cp, nsrc, SEED) if nsrc else np.zeros(0, np.uint32)
-    t1 = time.time()
-    ref = O.RefGraph.from_csc(n, cp, rw)
-    del cp, rw
-    social = ref.is_social()
-    inv = ref.reorder(order, window or 65536)
-    t2 = time.time()
+    meta = Path(str(tag) + ".json")
+    if meta.exists():
+        info = json.loads(meta.read_text())
+        ref = O.RefGraph.load_csc(str(tag) + "_csc.bin")
+        social = bool(info["social"])
+        src = np.load(str(tag) + f"_sources{nsrc}.npy") if nsrc else np.zeros(0, np.uint32)
+        t1 = t2 = time.time()
+    else:
+        n, cp, rw = generate_oracle(gen)
+        samples = {k: O.sample_sources(n, cp, k, SEED) for k in counts}
+        t1 = time.time()
+        ref = O.RefGraph.from_csc(n, cp, rw)
+        del cp, rw
+        social = ref.is_social()
+        inv = ref.reorder(order, window or 65536)
+        t2 = time.time()
+        ref.save_csc(str(tag) + "_csc.bin")
+        for k, sk in samples.items():
+            np.save(str(tag) + f"_sources{k}.npy", inv[sk].astype(np.uint32))
+        meta.write_text(json.dumps({"social": social}))
+        src = inv[samples[nsrc]] if nsrc else np.zeros(0, np.uint32)
     ref.build_bvss(full_padding=not social)
     t3 = time.time()
-    _, nnz, rcp, rrw = ref.csc()
+    n, nnz, rcp, rrw = ref.csc()
     slices = int(ref.bvss_slices())
     log(f"[prep:reference] {workload}: generate {t1 - t0:.1f}s reorder {t2 - t1:.1f}s bvss {t3 - t2:.1f}s "
         f"n={n} nnz={nnz} social={social} slices={slices}")
-    return ref, n, nnz, rcp, rrw, inv[src] if len(src) else src, slices
+    return ref, n, nnz, rcp, rrw, np.asarray(src, dtype=np.uint32), slices
 
 
 def run_reference(args, rank, world):
@@ -1210,7 +1229,7 @@ def run_reference(args, rank, world):
         return {"impl": "reference", "unavailable": "the reference has no multi-source BFS or serving implementation "
                                                     "(MBFS/BVSSMBFSKernel.cuh is empty; no server)"}
     dev = int(os.environ.get("LOCAL_RANK", "0"))
-    ref, n, nnz, cp, rw, sources, slices = prepare_reference(args.workload)
+    ref, n, nnz, cp, rw, sources, slices = prepare_reference(args.workload, Path(args.cache))
     deg = np.diff(cp.astype(np.int64))
     variant = ["BVSSBFS8EnhancedSliceSize8NoMasks4", "FullPad", "LazySwitching", "LazyFullPad"][ref.bfs_variant()]
     if kind == "cc":
