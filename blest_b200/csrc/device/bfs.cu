@@ -589,6 +589,7 @@ __device__ __forceinline__ void bfs_run(const BfsArgs& a) {
                 // registers to software-pipeline the steps: the tile loads
                 // of step s + 1 are in flight while step s's hit rows are
                 // checked and ORed.
+                const bool lazy_check = D1 > (uint64_t)(g.n / 8);
                 StepLoad cur = load_step<ALIGNED>(a, qw, U1, U2 + s * per, c);
                 for (; s < send; ++s) {
                     const bool more = s + 1 < send;  // warp-uniform
@@ -601,11 +602,16 @@ __device__ __forceinline__ void bfs_run(const BfsArgs& a) {
                     if (hits) {
                         const uint32_t rowk[4] = {cur.rows.x, cur.rows.y, cur.rows.z, cur.rows.w};
                         // the hit rows' visited words first (independent loads
-                        // in flight together), then the ORs
+                        // in flight together), then the ORs; while under an
+                        // eighth of the graph is visited the check filters
+                        // few ORs and only adds a round trip per step (the
+                        // sweep drops visited candidates either way)
                         uint32_t vis[4];
 #pragma unroll
                         for (uint32_t kk = 0; kk < 4; ++kk)
-                            vis[kk] = ((hits >> kk) & 1u) && rowk[kk] < g.n ? __ldcg(&a.visited[rowk[kk] >> 5]) : 0u;
+                            vis[kk] = lazy_check && ((hits >> kk) & 1u) && rowk[kk] < g.n
+                                          ? __ldcg(&a.visited[rowk[kk] >> 5])
+                                          : 0u;
 #pragma unroll
                         for (uint32_t kk = 0; kk < 4; ++kk) {
                             if (!((hits >> kk) & 1u)) continue;
