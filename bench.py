@@ -714,11 +714,20 @@ def run_serving(args, rank, world):
     import queue as qmod
 
     def make_pools(device: bool):
+        """Result buffers per graph: enough that the client rarely waits for
+        one (it waits only when every buffer of a graph holds a request in
+        flight), capped per graph at --pool-gb of device memory, or
+        --host-pool-gb of pinned host memory (at most a quarter of the
+        host's available RAM over all graphs)."""
+        if device:
+            cap = args.pool_gb * 1e9
+        else:
+            import psutil
+            cap = min(args.host_pool_gb * 1e9, 0.25 * psutil.virtual_memory().available / len(graphs))
         pools = []
         for _, csc, _, _, _ in graphs:
             q = qmod.Queue()
-            # at most ~2 GB of result buffers per graph
-            for _ in range(max(8, min(args.buffers, int(2e9 // (4 * csc.n))))):
+            for _ in range(max(8, min(args.buffers, int(cap // (4 * csc.n))))):
                 if device:
                     q.put(torch.empty(csc.n, dtype=torch.int32, device="cuda"))
                 else:
@@ -776,41 +785,58 @@ def run_serving(args, rank, world):
 
 
 def serving_sweep(args, graphs, pools, rates, Server):
-    """Open-loop Poisson arrivals at each rate; returns one record per rate."""
+    """Open-loop Poisson arrivals at each rate; returns one record per rate.
+
+    Request i is due at its Poisson arrival time; the client submits it then
+    (or, if every result buffer of its graph is in flight, as soon as one is
+    recycled: the wait is counted as client stall and as latency). A
+    consumer thread takes finished tickets from the server's completion
+    queue in completion order and recycles their buffers at once. Latency
+    p50/p99 run from the due time to completion (open loop); the server's
+    own figures (from submission) are reported beside them."""
     import threading
     rng = np.random.default_rng(SEED)
     sweep = []
     for lam in rates:
-        srv = Server(lanes=args.lanes, max_batch=128)
+        srv = Server(lanes=args.lanes, max_batch=128, completion_queue=True)
         gids = [srv.add_graph(g) for _, _, g, _, _ in graphs]
         nreq = int(min(args.requests, max(50, lam * args.seconds)))
         gaps = rng.exponential(1.0 / lam, nreq)
         kinds = rng.random(nreq) < 0.8
         which = rng.integers(0, len(graphs), nreq)
-        tickets = []
-        edges = [0]
+        inflight = {}  # ticket id -> (graph index, pool source index, buffer, client delay s)
         lock = threading.Lock()
+        lat, edges, failed = [], [0], [0]
+        left = [nreq]
 
-        def consume(queue):
+        def consume():
             while True:
-                item = queue.pop(0) if queue else None
-                if item is None:
-                    if done_flag[0] and not queue:
+                with lock:
+                    if left[0] == 0:
                         return
-                    time.sleep(0.0005)
+                got = srv.next_done(0.05)
+                if got is None:
                     continue
-                t, gi, si = item
-                t.result(600)
-                if si >= 0:
-                    with lock:
+                tid, info = got
+                with lock:
+                    while tid not in inflight:  # submit() returned but not yet recorded
+                        lock.release()
+                        time.sleep(0)
+                        lock.acquire()
+                    gi, si, buf, delay = inflight.pop(tid)
+                    left[0] -= 1
+                if info.status != 0:
+                    failed[0] += 1
+                else:
+                    lat.append(info.done_s - info.submit_s + delay)
+                    if si >= 0:
                         edges[0] += int(graphs[gi][3][si])
-                pools[gi].put(t.out)
-                t.out = None
+                pools[gi].put(buf)
+                srv.release(tid)
 
-        queue = []
-        done_flag = [False]
-        cons = threading.Thread(target=consume, args=(queue,))
+        cons = threading.Thread(target=consume)
         cons.start()
+        stall = 0.0
         t_start = time.perf_counter()
         due = t_start
         for i in range(nreq):
@@ -818,26 +844,40 @@ def serving_sweep(args, graphs, pools, rates, Server):
             while time.perf_counter() < due:
                 pass
             gi = int(which[i])
-            buf = pools[gi].get()
+            try:
+                buf = pools[gi].get_nowait()
+            except Exception:
+                t0 = time.perf_counter()
+                buf = pools[gi].get()
+                stall += time.perf_counter() - t0
             si = -1
-            if kinds[i]:
-                src = graphs[gi][4]
-                si = int(rng.integers(0, len(src)))
-                t = srv.submit_bfs(gids[gi], int(src[si]), out=buf)
-            else:
-                t = srv.submit_cc(gids[gi], out=buf)
-            tickets.append(t)
-            queue.append((t, gi, si))
+            with lock:
+                if kinds[i]:
+                    src = graphs[gi][4]
+                    si = int(rng.integers(0, len(src)))
+                    t = srv.submit_bfs(gids[gi], int(src[si]), out=buf)
+                else:
+                    t = srv.submit_cc(gids[gi], out=buf)
+                inflight[t.id] = (gi, si, buf, time.perf_counter() - due)
         srv.drain(600)
         wall = time.perf_counter() - t_start
-        done_flag[0] = True
         cons.join()
         st = srv.stats()
+        lat_ms = np.sort(np.array(lat)) * 1e3
+        pct = lambda q: round(float(lat_ms[min(len(lat_ms) - 1, int(q * (len(lat_ms) - 1) + 0.5))]), 3)
         sweep.append({"rate_per_s": lam, "requests": nreq, "wall_s": round(wall, 3),
                       "throughput_per_s": round(nreq / wall, 1),
-                      "p50_ms": round(st["p50_latency_s"] * 1e3, 3), "p99_ms": round(st["p99_latency_s"] * 1e3, 3),
-                      "mean_ms": round(st["mean_latency_s"] * 1e3, 3), "jobs": st["jobs"],
+                      "p50_ms": pct(0.50), "p99_ms": pct(0.99), "mean_ms": round(float(lat_ms.mean()), 3),
+                      "server_p50_ms": round(st["p50_latency_s"] * 1e3, 3),
+                      "server_p99_ms": round(st["p99_latency_s"] * 1e3, 3),
+                      "client_stall_s": round(stall, 3), "jobs": st["jobs"],
                       "batched_requests": st["batched_requests"], "rejected": st["rejected"],
+                      "failed": failed[0],
+                      "jobs_by_kind": {"bfs": st["jobs_bfs"], "mbfs": st["jobs_mbfs"], "cc": st["jobs_cc"]},
+                      "requests_by_kind": {"bfs": st["jobs_bfs"], "mbfs": st["requests_mbfs"],
+                                           "cc": st["requests_cc"]},
+                      "lane_busy_s": {"bfs": round(st["busy_bfs_s"], 3), "mbfs": round(st["busy_mbfs_s"], 3),
+                                      "cc": round(st["busy_cc_s"], 3)},
                       "bfs_gteps": round(edges[0] / wall / 1e9, 3)})
         log(f"[serving] rate {lam}/s: {sweep[-1]}")
         srv.close()
@@ -1360,7 +1400,12 @@ def main():
     ap.add_argument("--seconds", type=float, default=2.0)
     ap.add_argument("--lanes", type=int, default=4)
     ap.add_argument("--serving-full", action="store_true")
-    ap.add_argument("--buffers", type=int, default=192)
+    ap.add_argument("--buffers", type=int, default=512,
+                    help="serving: most result buffers per graph")
+    ap.add_argument("--pool-gb", type=float, default=8.0,
+                    help="serving: most GB of device result buffers per graph")
+    ap.add_argument("--host-pool-gb", type=float, default=3.0,
+                    help="serving: most GB of pinned host result buffers per graph")
     ap.add_argument("--serving-results", choices=["host", "device", "both"], default="both",
                     help="serving: result buffers in pinned host memory, device memory, or a sweep of each")
     ap.add_argument("--autotune", action="store_true", help="tune BFS launch parameters before timing")

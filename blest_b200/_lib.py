@@ -114,7 +114,7 @@ class MbfsStats(C.Structure):
 
 class ServerParams(C.Structure):
     _fields_ = [("memory_budget", u64), ("lanes", u32), ("max_batch", u32), ("queue_capacity", u32),
-                ("dry_run", i32)]
+                ("dry_run", i32), ("completion_queue", i32)]
 
 
 class QueryResult(C.Structure):
@@ -125,7 +125,9 @@ class QueryResult(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [("submitted", u64), ("completed", u64), ("rejected", u64), ("jobs", u64),
                 ("batched_requests", u64), ("p50_latency_s", f64), ("p99_latency_s", f64),
-                ("mean_latency_s", f64), ("busy_s", f64), ("peak_reserved_bytes", u64), ("memory_budget", u64)]
+                ("mean_latency_s", f64), ("busy_s", f64), ("peak_reserved_bytes", u64), ("memory_budget", u64),
+                ("jobs_bfs", u64), ("jobs_mbfs", u64), ("jobs_cc", u64), ("requests_mbfs", u64),
+                ("requests_cc", u64), ("busy_bfs_s", f64), ("busy_mbfs_s", f64), ("busy_cc_s", f64)]
 
 
 class MbfsItem(C.Structure):
@@ -197,6 +199,7 @@ _SIGS = {
     "blest_mbfs": [vp, P(u32), u32, vp, i32, P(MbfsParams), P(MbfsStats)],
     "blest_mbfs_batch": [P(MbfsItem), u32, i32, P(MbfsParams), vp, P(MbfsStats)],
     "blest_mbfs_ws": [vp, P(u32), u32, vp, i32, P(MbfsParams), vp, P(MbfsStats)],
+    "blest_mbfs_rows_ws": [vp, P(u32), u32, P(vp), P(MbfsParams), vp, P(MbfsStats)],
     "blest_mbfs_plan_create": [P(MbfsItem), u32, P(MbfsParams), vp, P(vp)],
     "blest_mbfs_plan_set_sources": [vp, u32, P(u32)],
     "blest_mbfs_plan_run": [vp, P(MbfsStats)],
@@ -213,6 +216,8 @@ _SIGS = {
     "blest_server_poll": [vp, u64, P(i32), P(QueryResult)],
     "blest_server_wait": [vp, u64, f64, P(QueryResult)],
     "blest_server_drain": [vp, f64],
+    "blest_server_next_done": [vp, f64, P(u64), P(QueryResult)],
+    "blest_server_release": [vp, u64],
     "blest_server_stats_get": [vp, P(ServerStats)],
     "blest_server_destroy": [vp],
 }

@@ -29,6 +29,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "../host/common.hpp"
@@ -78,6 +79,9 @@ struct MbfsArgs {
     const uint32_t* sources;   // local source ids, per part from src_base
     uint32_t* part_nf;         // 2 slots x nparts: vertices found per part at the last two levels
     blest_level_trace* trace;  // optional: one record per level of every group
+    // Single-graph runs only: when set, source i's levels go to rows[i]
+    // (one caller buffer of n words per source) instead of part0.levels.
+    uint32_t* const* rows;
     uint32_t groups;           // ceil(max k / group_width)
     uint32_t group_width;      // sources per group (32 * WORDS)
     float pull_fraction;       // pull when frontier vertices > n * pull_fraction
@@ -291,7 +295,15 @@ __device__ __forceinline__ void write_levels(const MbfsArgs& a, uint32_t warp, u
                 }
                 if (final) vis = __ldcg(a.visited + (size_t)v * WORDS + w);
             }
+            // with a rows table, lane j holds the buffer of the word's j-th
+            // source, handed to the warp by shuffle (rw is warp-uniform)
+            uint32_t* mine = nullptr;
+            if (a.rows && lane < rw) mine = a.rows[s0 + 32u * w + lane];
             for (uint32_t bit = 0; bit < rw; ++bit) {
+                uint32_t* const dst =
+                    a.rows ? reinterpret_cast<uint32_t*>(
+                                 __shfl_sync(0xFFFFFFFFu, reinterpret_cast<unsigned long long>(mine), bit))
+                           : P.levels + (uint64_t)(s0 + 32u * w + bit) * P.n;
                 uint32_t lvl;
                 if ((found >> bit) & 1u) {
                     uint32_t rel = 0;
@@ -303,7 +315,7 @@ __device__ __forceinline__ void write_levels(const MbfsArgs& a, uint32_t warp, u
                 } else {
                     continue;
                 }
-                if (in) P.levels[(uint64_t)(s0 + 32u * w + bit) * P.n + lv] = lvl;
+                if (in) dst[lv] = lvl;
             }
         }
     });
@@ -682,8 +694,9 @@ struct MbfsScratch {
     uint32_t* queue = nullptr;  // rset queue: 2 slots of entries + 2 slots of offsets
     uint32_t* part_nf = nullptr;  // per-graph frontier counts, 2 slots
     uint32_t* part_last = nullptr;  // per-graph last level with a valid history slot
+    uint32_t* rows = nullptr;  // per-source output pointers (2 words each)
     size_t state_words = 0, levels_words = 0, sources_cap = 0, queue_words = 0, part_nf_cap = 0,
-           part_last_cap = 0;
+           part_last_cap = 0, rows_words = 0;
 };
 
 // Entries one queue slot needs: a sweep queues each rset at most once; the
@@ -797,6 +810,7 @@ void mbfs_scratch_free(void* p) {
     cudaFree(sc->queue);
     cudaFree(sc->part_nf);
     cudaFree(sc->part_last);
+    cudaFree(sc->rows);
     delete sc;
 }
 
@@ -1002,61 +1016,95 @@ void check_sources(const blest_mbfs_item& it, uint32_t n) {
 
 }  // namespace
 
+namespace {
+
+// One single-graph run on `ws`: levels to `levels_out` (source-major, host
+// or device) or, with `rows`, to one device buffer per source.
+void mbfs_single(blest_workspace* ws, const uint32_t* sources, uint32_t k, uint32_t* levels_out, int out_mem,
+                 uint32_t* const* rows, const blest_mbfs_params* params, void* stream, blest_mbfs_stats* stats) {
+    blest::require(ws && sources && (levels_out || rows), "null argument");
+    blest::require(out_mem == BLEST_MEM_HOST || out_mem == BLEST_MEM_DEVICE, "bad out_mem");
+    const blest_graph* g = ws->g;
+    const uint32_t n = g->d.n;
+    for (uint32_t i = 0; i < k; ++i)
+        if (sources[i] >= n) throw blest::Error(BLEST_ERR_INVALID_ARG, "source vertex out of range");
+    if (k == 0) return;
+    blest_mbfs_params p{};
+    if (params) p = *params;
+    const uint32_t gw = p.group_width ? p.group_width : 128;
+    blest::require(gw == 32 || gw == 64 || gw == 128, "group_width must be 32, 64 or 128");
+    BLEST_CUDA(cudaSetDevice(g->device));
+    for (uint32_t i = 0; rows && i < k; ++i) {
+        cudaPointerAttributes at{};
+        BLEST_CUDA(cudaPointerGetAttributes(&at, rows[i]));
+        if (!rows[i] || !((at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) &&
+                          at.device == g->device))
+            throw blest::Error(BLEST_ERR_INVALID_ARG,
+                               "rows[" + std::to_string(i) + "] is not memory of the workspace's device");
+    }
+    cudaStream_t s = stream ? (cudaStream_t)stream : g->stream;
+    blest::Workspace& w = ws->w;
+    if (!w.mbfs) w.mbfs = new blest::MbfsScratch;
+    blest::MbfsScratch& sc = *(blest::MbfsScratch*)w.mbfs;
+    blest::ensure(sc.sources, sc.sources_cap, k);
+    BLEST_CUDA(cudaMemcpyAsync(sc.sources, sources, 4ull * k, cudaMemcpyHostToDevice, s));
+    uint32_t* dl = levels_out;
+    if (rows) {
+        // pageable source: the call returns once the table is staged
+        blest::ensure(sc.rows, sc.rows_words, 2ull * k);
+        BLEST_CUDA(cudaMemcpyAsync(sc.rows, rows, sizeof(uint32_t*) * k, cudaMemcpyHostToDevice, s));
+        dl = nullptr;
+    } else if (out_mem == BLEST_MEM_HOST) {
+        blest::ensure(sc.levels, sc.levels_words, (size_t)k * n);
+        dl = sc.levels;
+    }
+    blest::MbfsLaunch L = blest::prepare_mbfs(g, w, sc, p, std::min(k, gw), 1);
+    L.a.parts = nullptr;
+    L.a.nparts = 1;
+    L.a.word_part = nullptr;
+    L.a.part0 = blest::dev::MbfsPart{0u, n, k, 0u, 0u, g->d.no_pull_chunks, dl};
+    L.a.rows = rows ? reinterpret_cast<uint32_t* const*>(sc.rows) : nullptr;
+    L.a.sources = sc.sources;
+    L.a.groups = (k + gw - 1) / gw;
+    BLEST_CUDA(cudaEventRecord(w.ev_start, s));
+    blest::issue_mbfs(L, s);
+    BLEST_CUDA(cudaEventRecord(w.ev_stop, s));
+    BLEST_CUDA(cudaMemcpyAsync(w.host_counters, w.counters, sizeof(blest::dev::RunCounters),
+                               cudaMemcpyDeviceToHost, s));
+    if (!rows && out_mem == BLEST_MEM_HOST)
+        BLEST_CUDA(cudaMemcpyAsync(levels_out, dl, 4ull * k * n, cudaMemcpyDeviceToHost, s));
+    BLEST_CUDA(cudaStreamSynchronize(s));
+    const blest::dev::RunCounters& c = *w.host_counters;
+    if (c.error)
+        throw blest::Error((int)c.error, c.error == BLEST_ERR_BARRIER_TIMEOUT ? "device grid barrier timed out"
+                                                                             : "MBFS device error");
+    float ms = 0;
+    BLEST_CUDA(cudaEventElapsedTime(&ms, w.ev_start, w.ev_stop));
+    if (stats) {
+        stats->time = ms * 1e-3;
+        stats->groups = (k + gw - 1) / gw;
+        stats->max_levels = c.levels + 1;
+        stats->reached_degree_sum = 0;
+    }
+}
+
+}  // namespace
+
 extern "C" {
 
 int blest_mbfs_ws(blest_workspace* ws, const uint32_t* sources, uint32_t k, uint32_t* levels_out, int out_mem,
                   const blest_mbfs_params* params, void* stream, blest_mbfs_stats* stats) {
     return guarded([&] {
-        blest::require(ws && sources && levels_out, "null argument");
-        blest::require(out_mem == BLEST_MEM_HOST || out_mem == BLEST_MEM_DEVICE, "bad out_mem");
-        const blest_graph* g = ws->g;
-        const uint32_t n = g->d.n;
-        for (uint32_t i = 0; i < k; ++i)
-            if (sources[i] >= n) throw blest::Error(BLEST_ERR_INVALID_ARG, "source vertex out of range");
-        if (k == 0) return;
-        blest_mbfs_params p{};
-        if (params) p = *params;
-        const uint32_t gw = p.group_width ? p.group_width : 128;
-        blest::require(gw == 32 || gw == 64 || gw == 128, "group_width must be 32, 64 or 128");
-        BLEST_CUDA(cudaSetDevice(g->device));
-        cudaStream_t s = stream ? (cudaStream_t)stream : g->stream;
-        blest::Workspace& w = ws->w;
-        if (!w.mbfs) w.mbfs = new blest::MbfsScratch;
-        blest::MbfsScratch& sc = *(blest::MbfsScratch*)w.mbfs;
-        blest::ensure(sc.sources, sc.sources_cap, k);
-        BLEST_CUDA(cudaMemcpyAsync(sc.sources, sources, 4ull * k, cudaMemcpyHostToDevice, s));
-        uint32_t* dl = levels_out;
-        if (out_mem == BLEST_MEM_HOST) {
-            blest::ensure(sc.levels, sc.levels_words, (size_t)k * n);
-            dl = sc.levels;
-        }
-        blest::MbfsLaunch L = blest::prepare_mbfs(g, w, sc, p, std::min(k, gw), 1);
-        L.a.parts = nullptr;
-        L.a.nparts = 1;
-        L.a.word_part = nullptr;
-        L.a.part0 = blest::dev::MbfsPart{0u, n, k, 0u, 0u, g->d.no_pull_chunks, dl};
-        L.a.sources = sc.sources;
-        L.a.groups = (k + gw - 1) / gw;
-        BLEST_CUDA(cudaEventRecord(w.ev_start, s));
-        blest::issue_mbfs(L, s);
-        BLEST_CUDA(cudaEventRecord(w.ev_stop, s));
-        BLEST_CUDA(cudaMemcpyAsync(w.host_counters, w.counters, sizeof(blest::dev::RunCounters),
-                                   cudaMemcpyDeviceToHost, s));
-        if (out_mem == BLEST_MEM_HOST)
-            BLEST_CUDA(cudaMemcpyAsync(levels_out, dl, 4ull * k * n, cudaMemcpyDeviceToHost, s));
-        BLEST_CUDA(cudaStreamSynchronize(s));
-        const blest::dev::RunCounters& c = *w.host_counters;
-        if (c.error)
-            throw blest::Error((int)c.error, c.error == BLEST_ERR_BARRIER_TIMEOUT ? "device grid barrier timed out"
-                                                                                 : "MBFS device error");
-        float ms = 0;
-        BLEST_CUDA(cudaEventElapsedTime(&ms, w.ev_start, w.ev_stop));
-        if (stats) {
-            stats->time = ms * 1e-3;
-            stats->groups = (k + gw - 1) / gw;
-            stats->max_levels = c.levels + 1;
-            stats->reached_degree_sum = 0;
-        }
+        blest::require(levels_out, "null argument");
+        mbfs_single(ws, sources, k, levels_out, out_mem, nullptr, params, stream, stats);
+    });
+}
+
+int blest_mbfs_rows_ws(blest_workspace* ws, const uint32_t* sources, uint32_t k, uint32_t* const* rows,
+                       const blest_mbfs_params* params, void* stream, blest_mbfs_stats* stats) {
+    return guarded([&] {
+        blest::require(rows, "null argument");
+        mbfs_single(ws, sources, k, nullptr, BLEST_MEM_DEVICE, rows, params, stream, stats);
     });
 }
 

@@ -14,8 +14,11 @@
 // Each lane has its own CUDA stream and per-graph workspaces whose
 // cooperative grids are capped to a share of the SMs, so jobs on different
 // lanes run side by side on the device. Results land in the caller's
-// buffer, host memory or (for a consumer on the GPU) device memory; each
-// request records submit / start / done times.
+// buffer, host memory or (for a consumer on the GPU) device memory: a
+// batch writes the device-bound results straight into their buffers (one
+// output row per source) and stages only the host-bound ones. Each request
+// records submit / start / done times; an optional completion queue hands
+// finished tickets to the client in completion order.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -96,9 +99,11 @@ struct blest_server {
     blest::Clock::time_point t0;
     int device = 0;
     uint32_t lane_grid = 0;
+    std::deque<uint64_t> done_q;  // finished tickets (completion_queue servers)
     // stats
     uint64_t submitted = 0, completed = 0, rejected = 0, jobs = 0, batched = 0;
-    double busy_s = 0;
+    uint64_t kind_jobs[3] = {0, 0, 0}, kind_requests[3] = {0, 0, 0};  // single BFS, multi-source BFS, CC
+    double busy_s = 0, kind_busy[3] = {0, 0, 0};
     std::vector<double> latencies;
 };
 
@@ -107,11 +112,20 @@ namespace {
 
 double now(const blest_server* s) { return std::chrono::duration<double>(Clock::now() - s->t0).count(); }
 
-// Device bytes a job needs beyond already-resident workspaces.
-uint64_t job_bytes(const GraphEntry& ge, int kind, uint32_t k) {
+// Job kinds for the per-kind statistics.
+int job_kind(const Job& job) {
+    return job.kind == BLEST_QUERY_CC ? 2 : (job.reqs.size() > 1 ? 1 : 0);
+}
+
+// Device bytes a job needs beyond already-resident workspaces: the MBFS
+// state and a staging row per host-bound result (device-bound results are
+// written straight into their buffers).
+uint64_t job_bytes(const GraphEntry& ge, int kind, const std::vector<Request*>& reqs, uint32_t k) {
     if (kind == BLEST_QUERY_CC || k <= 1) return 0;
     const uint64_t words = k <= 32 ? 1 : (k <= 64 ? 2 : 4);
-    return 4ull * mbfs_state_words(ge.n, (uint32_t)words) + 4ull * k * ge.n;  // MBFS state + staged levels
+    uint64_t host = 0;
+    for (uint32_t i = 0; i < k && i < reqs.size(); ++i) host += reqs[i]->out_mem == BLEST_MEM_HOST;
+    return 4ull * mbfs_state_words(ge.n, (uint32_t)words) + 4ull * host * ge.n;
 }
 
 void finish(blest_server* s, Job& job, int status, const std::string& err, double start) {
@@ -126,7 +140,12 @@ void finish(blest_server* s, Job& job, int status, const std::string& err, doubl
         r->done = true;
         ++s->completed;
         s->latencies.push_back(t - r->submit);
+        if (s->p.completion_queue) s->done_q.push_back(r->id);
     }
+    const int kk = job_kind(job);
+    ++s->kind_jobs[kk];
+    s->kind_requests[kk] += job.reqs.size();
+    s->kind_busy[kk] += t - start;
     s->reserved -= job.bytes;
     s->busy_s += t - start;
 }
@@ -163,24 +182,32 @@ int run_job(blest_server* s, Lane& lane, Job& job) {
     if (job.reqs.size() == 1)
         return blest_bfs_ws(ws, job.reqs[0]->source, job.reqs[0]->out, nullptr, job.reqs[0]->out_mem, nullptr,
                             lane.stream, 0, nullptr);
+    // one output row per source: a device-bound result's own buffer, or a
+    // staging row for a host-bound one (copied out after the run)
     const uint32_t k = (uint32_t)job.reqs.size();
     std::vector<uint32_t> src(k);
-    for (uint32_t i = 0; i < k; ++i) src[i] = job.reqs[i]->source;
+    std::vector<uint32_t*> rows(k);
+    uint32_t host = 0;
+    for (uint32_t i = 0; i < k; ++i) {
+        src[i] = job.reqs[i]->source;
+        host += job.reqs[i]->out_mem == BLEST_MEM_HOST;
+    }
     blest_mbfs_params mp{};
     mp.group_width = k <= 32 ? 32 : (k <= 64 ? 64 : 128);
     uint32_t* staging = nullptr;
-    if (cudaMallocAsync((void**)&staging, 4ull * k * ge.n, lane.stream) != cudaSuccess) {
+    if (host && cudaMallocAsync((void**)&staging, 4ull * host * ge.n, lane.stream) != cudaSuccess) {
         cudaGetLastError();
         return BLEST_ERR_OOM;
     }
-    int rc = blest_mbfs_ws(ws, src.data(), k, staging, BLEST_MEM_DEVICE, &mp, lane.stream, nullptr);
-    if (rc == BLEST_OK) {
-        for (uint32_t i = 0; i < k && rc == BLEST_OK; ++i)
-            if (cudaMemcpyAsync(job.reqs[i]->out, staging + (size_t)i * ge.n, 4ull * ge.n, cudaMemcpyDefault,
-                                lane.stream) != cudaSuccess)
-                rc = BLEST_ERR_CUDA;
-    }
-    cudaFreeAsync(staging, lane.stream);
+    for (uint32_t i = 0, h = 0; i < k; ++i)
+        rows[i] = job.reqs[i]->out_mem == BLEST_MEM_HOST ? staging + (size_t)(h++) * ge.n : job.reqs[i]->out;
+    int rc = blest_mbfs_rows_ws(ws, src.data(), k, rows.data(), &mp, lane.stream, nullptr);
+    for (uint32_t i = 0; i < k && rc == BLEST_OK; ++i)
+        if (job.reqs[i]->out_mem == BLEST_MEM_HOST &&
+            cudaMemcpyAsync(job.reqs[i]->out, rows[i], 4ull * ge.n, cudaMemcpyDeviceToHost, lane.stream) !=
+                cudaSuccess)
+            rc = BLEST_ERR_CUDA;
+    if (staging) cudaFreeAsync(staging, lane.stream);
     if (cudaStreamSynchronize(lane.stream) != cudaSuccess && rc == BLEST_OK) rc = BLEST_ERR_CUDA;
     return rc;
 }
@@ -222,9 +249,9 @@ bool form_job(blest_server* s, Job& job) {
     // shrink the batch until it fits the memory that is free now
     uint32_t k = (uint32_t)take.size();
     if (job.kind == BLEST_QUERY_BFS) {
-        while (k > 1 && s->reserved + job_bytes(ge, job.kind, k) > s->budget) k = k > 32 ? (k + 1) / 2 : k - 1;
+        while (k > 1 && s->reserved + job_bytes(ge, job.kind, take, k) > s->budget) k = k > 32 ? (k + 1) / 2 : k - 1;
     }
-    const uint64_t need = job_bytes(ge, job.kind, job.kind == BLEST_QUERY_BFS ? k : 1);
+    const uint64_t need = job_bytes(ge, job.kind, take, job.kind == BLEST_QUERY_BFS ? k : 1);
     if (s->reserved + need > s->budget) return false;
     take.resize(job.kind == BLEST_QUERY_BFS ? k : take.size());
     job.reqs = take;
@@ -263,6 +290,7 @@ void scheduler_main(blest_server* s) {
                 r->done = true;
                 r->done_t = now(s);
                 ++s->rejected;
+                if (s->p.completion_queue) s->done_q.push_back(r->id);
                 s->cv_done.notify_all();
                 continue;
             }
@@ -443,6 +471,33 @@ int blest_server_drain(blest_server* s, double timeout_s) {
     });
 }
 
+int blest_server_next_done(blest_server* s, double timeout_s, uint64_t* ticket, blest_query_result* result) {
+    return guarded([&] {
+        blest::require(s && ticket, "null argument");
+        blest::require(s->p.completion_queue, "server was created without a completion queue");
+        *ticket = 0;
+        std::unique_lock<std::mutex> lk(s->mu);
+        const bool ok = s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s),
+                                            [&] { return !s->done_q.empty(); });
+        if (!ok) throw blest::Error(BLEST_ERR_BUSY, "no request finished within the timeout");
+        *ticket = s->done_q.front();
+        s->done_q.pop_front();
+        auto it = s->requests.find(*ticket);
+        if (it != s->requests.end()) fill_result(*it->second, result);
+    });
+}
+
+int blest_server_release(blest_server* s, uint64_t ticket) {
+    return guarded([&] {
+        blest::require(s, "null argument");
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto it = s->requests.find(ticket);
+        blest::require(it != s->requests.end(), "unknown ticket");
+        blest::require(it->second->done, "request has not finished");
+        s->requests.erase(it);
+    });
+}
+
 int blest_server_stats_get(blest_server* s, blest_server_stats* out) {
     return guarded([&] {
         blest::require(s && out, "null argument");
@@ -456,6 +511,14 @@ int blest_server_stats_get(blest_server* s, blest_server_stats* out) {
         out->busy_s = s->busy_s;
         out->peak_reserved_bytes = s->peak;
         out->memory_budget = s->budget;
+        out->jobs_bfs = s->kind_jobs[0];
+        out->jobs_mbfs = s->kind_jobs[1];
+        out->jobs_cc = s->kind_jobs[2];
+        out->requests_mbfs = s->kind_requests[1];
+        out->requests_cc = s->kind_requests[2];
+        out->busy_bfs_s = s->kind_busy[0];
+        out->busy_mbfs_s = s->kind_busy[1];
+        out->busy_cc_s = s->kind_busy[2];
         std::vector<double> l = s->latencies;
         if (!l.empty()) {
             std::sort(l.begin(), l.end());

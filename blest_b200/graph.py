@@ -467,6 +467,18 @@ class Workspace:
         L.call("blest_cc_ws", self._h, labels_ptr, out_mem, stream, C.byref(st))
         return CcStats(st.time, st.no_components, st.iterations)
 
+    def mbfs_rows(self, sources, rows, group_width: int = 128, stream: int = 0) -> MbfsStats:
+        """Blocking multi-source BFS with one device buffer per source:
+        rows[i] (a device pointer as int) receives the n levels of
+        sources[i] (blest_mbfs_rows_ws)."""
+        src = np.ascontiguousarray(sources, dtype=np.uint32)
+        assert len(rows) == src.size
+        ptrs = (C.c_void_p * max(1, src.size))(*rows)
+        p = L.MbfsParams(group_width, 0, 0, 0.0, 0)
+        st = L.MbfsStats()
+        L.call("blest_mbfs_rows_ws", self._h, _u32p(src), src.size, ptrs, C.byref(p), stream, C.byref(st))
+        return MbfsStats(st.time, st.groups, st.max_levels, st.reached_degree_sum)
+
 
 class MbfsPlan:
     """Multi-graph multi-source BFS in one persistent launch, replayed from a

@@ -5,6 +5,10 @@
     t = srv.submit_bfs(gid, source)            # returns a Ticket
     levels = t.result()                        # numpy uint32[n]
     srv.stats()                                # p50 / p99 latency, jobs, batching
+
+With completion_queue=True, srv.next_done() returns finished tickets in
+completion order, so a client can reuse each result buffer as soon as its
+request is done.
 """
 from __future__ import annotations
 
@@ -59,8 +63,8 @@ class Ticket:
 
 class Server:
     def __init__(self, lanes: int = 4, max_batch: int = 128, memory_budget: int = 0, queue_capacity: int = 0,
-                 dry_run: bool = False):
-        p = L.ServerParams(memory_budget, lanes, max_batch, queue_capacity, int(dry_run))
+                 dry_run: bool = False, completion_queue: bool = False):
+        p = L.ServerParams(memory_budget, lanes, max_batch, queue_capacity, int(dry_run), int(completion_queue))
         h = C.c_void_p()
         L.call("blest_server_create", C.byref(p), C.byref(h))
         self._h = h
@@ -113,6 +117,22 @@ class Server:
 
     def submit_cc(self, gid: int, out: np.ndarray | None = None) -> Ticket:
         return self._submit(gid, L.QUERY_CC, 0, out)
+
+    def next_done(self, timeout_s: float = 600.0) -> tuple[int, QueryInfo] | None:
+        """(ticket id, QueryInfo) of the next request to finish or be refused
+        (servers made with completion_queue=True); None on timeout."""
+        t = L.u64()
+        r = L.QueryResult()
+        rc = L.fn["blest_server_next_done"](self._h, timeout_s, C.byref(t), C.byref(r))
+        if rc == L.ERR_BUSY:
+            return None
+        L.check(rc)
+        return t.value, QueryInfo(r.status, {0: "bfs", 1: "cc"}.get(r.kind, "?"), r.graph_id, r.source,
+                                  r.batch_size, r.submit_s, r.start_s, r.done_s)
+
+    def release(self, ticket: int) -> None:
+        """Forget a finished request's record."""
+        L.call("blest_server_release", self._h, ticket)
 
     def drain(self, timeout_s: float = 600.0) -> None:
         L.call("blest_server_drain", self._h, timeout_s)

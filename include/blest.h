@@ -411,6 +411,14 @@ int blest_mbfs(blest_graph* g, const uint32_t* sources, uint32_t k, uint32_t* le
 /* Same on an explicit workspace and stream (blocking). */
 int blest_mbfs_ws(blest_workspace* ws, const uint32_t* sources, uint32_t k, uint32_t* levels_out, int out_mem,
                   const blest_mbfs_params* params, void* stream, blest_mbfs_stats* stats);
+/* Same with one output buffer per source: rows (a host array of k
+ * pointers) gives for source i a device buffer of n uint32 on the
+ * workspace's device, and the kernel writes source i's levels straight into
+ * it (no source-major staging array, no copy). The query server uses it
+ * for coalesced requests whose results stay on the device. Buffers that
+ * are not device memory of the workspace's device: BLEST_ERR_INVALID_ARG. */
+int blest_mbfs_rows_ws(blest_workspace* ws, const uint32_t* sources, uint32_t k, uint32_t* const* rows,
+                       const blest_mbfs_params* params, void* stream, blest_mbfs_stats* stats);
 
 /* Many graphs, many sources, one persistent launch. The items' graphs are
  * joined on the device into one block-diagonal graph (each graph's vertices
@@ -468,8 +476,9 @@ int blest_mbfs_plan_destroy(blest_mbfs_plan* plan);
  * admitted when its device scratch fits the memory budget: the batch
  * shrinks or the job waits for running jobs to finish; a request that can
  * never fit is refused with BLEST_ERR_ADMISSION. Results land in the
- * caller's host buffer (n uint32 levels or labels). Graphs stay owned by
- * the caller and must outlive the server. */
+ * caller's buffer (n uint32 levels or labels), in host or device memory; a
+ * batch writes the results bound for device buffers straight into them.
+ * Graphs stay owned by the caller and must outlive the server. */
 typedef struct blest_server blest_server;
 #define BLEST_QUERY_BFS 0
 #define BLEST_QUERY_CC 1
@@ -480,6 +489,8 @@ typedef struct blest_server_params {
     uint32_t queue_capacity;  /* pending requests; 0 = 2^20 (BLEST_ERR_BUSY beyond) */
     int dry_run;              /* != 0: no GPU; jobs finish at once and out[0] = batch size
                                  (exercises the scheduling logic) */
+    int completion_queue;     /* != 0: every finished or refused request's ticket is also
+                                 queued for blest_server_next_done */
 } blest_server_params;
 typedef struct blest_query_result {
     int status;               /* BLEST_OK or the error code of the request */
@@ -499,6 +510,10 @@ typedef struct blest_server_stats {
     double busy_s;            /* summed lane busy time */
     uint64_t peak_reserved_bytes;
     uint64_t memory_budget;
+    /* per kind of GPU job: single-source BFS, coalesced multi-source BFS, CC */
+    uint64_t jobs_bfs, jobs_mbfs, jobs_cc;
+    uint64_t requests_mbfs, requests_cc;  /* requests those jobs served */
+    double busy_bfs_s, busy_mbfs_s, busy_cc_s;
 } blest_server_stats;
 int blest_server_create(const blest_server_params* p, blest_server** out);
 int blest_server_add_graph(blest_server* s, blest_graph* g, uint32_t* graph_id);
@@ -515,6 +530,14 @@ int blest_server_poll(blest_server* s, uint64_t ticket, int* done, blest_query_r
 int blest_server_wait(blest_server* s, uint64_t ticket, double timeout_s, blest_query_result* result);
 /* Wait until every submitted request has finished or been refused. */
 int blest_server_drain(blest_server* s, double timeout_s);
+/* Servers created with completion_queue: the ticket of the next request to
+ * finish (or be refused), in completion order, with its result record;
+ * BLEST_ERR_BUSY when none finishes within timeout_s. Lets a client recycle
+ * each result buffer as soon as its request is done, whatever the order. */
+int blest_server_next_done(blest_server* s, double timeout_s, uint64_t* ticket, blest_query_result* result);
+/* Forget a finished request (its ticket becomes unknown), so a long-running
+ * server does not keep a record of every request it has served. */
+int blest_server_release(blest_server* s, uint64_t ticket);
 int blest_server_stats_get(blest_server* s, blest_server_stats* out);
 int blest_server_destroy(blest_server* s);
 

@@ -77,6 +77,35 @@ def test_dry_run_validation_and_threads():
     assert all(t.done() for t in out)
 
 
+def test_dry_run_completion_queue_release_and_kind_stats():
+    srv = Server(lanes=2, max_batch=16, dry_run=True, completion_queue=True)
+    g = srv.add_virtual_graph(1000)
+    ts = [srv.submit_bfs(g, i) for i in range(50)] + [srv.submit_cc(g) for _ in range(4)]
+    seen = {}
+    while len(seen) < len(ts):
+        got = srv.next_done(30)
+        assert got is not None
+        tid, info = got
+        assert tid not in seen and info.status == 0
+        seen[tid] = info
+        srv.release(tid)
+    assert sorted(seen) == sorted(t.id for t in ts)
+    # completion order: done times never go backwards
+    done = [i.done_s for i in seen.values()]
+    assert done == sorted(done)
+    assert srv.next_done(0.01) is None  # nothing left: times out
+    with pytest.raises(BlestError):
+        srv.release(ts[0].id)  # already released: unknown ticket
+    st = srv.stats()
+    assert st["jobs"] == st["jobs_bfs"] + st["jobs_mbfs"] + st["jobs_cc"]
+    assert st["jobs_bfs"] + st["requests_mbfs"] == 50 and st["requests_cc"] == 4
+    assert st["jobs_mbfs"] >= 1 and st["busy_mbfs_s"] > 0
+    # without a completion queue, next_done is refused
+    srv2 = Server(lanes=1, dry_run=True)
+    with pytest.raises(BlestError):
+        srv2.next_done(0.01)
+
+
 @pytest.mark.gpu
 def test_results_equal_alone_and_in_the_mix(gpu):
     import oracle as O
@@ -146,6 +175,43 @@ def test_device_results_equal_host_results(gpu):
     assert batched > 0
     assert tc.info().status == 0
     np.testing.assert_array_equal(cc_out.cpu().numpy().view(np.uint32), O.cc_csc(csc.n, csc.col_ptrs, csc.rows))
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_batch_with_host_and_device_results(gpu):
+    """One coalesced batch whose results go partly to device buffers
+    (written by the kernel straight into them) and partly to host buffers
+    (staged, then copied): every result equals the oracle's; finished
+    tickets come back through the completion queue."""
+    import torch
+    import oracle as O
+    from blest_b200 import Csc, Graph
+    from graphs import prepared
+    csc, bvss, csr = prepared(Csc.er(3001, 12000, seed=6), "rcm", 4096)
+    g = Graph(bvss, csr)
+    srv = Server(lanes=1, max_batch=128, completion_queue=True)
+    gid = srv.add_graph(g)
+    srcs = [int(x) for x in csc.sample_sources(70, seed=5)]
+    # a first request occupies the lane while the rest queue up into one batch
+    first = srv.submit_cc(gid)
+    outs, tickets = [], []
+    for i, s in enumerate(srcs):
+        o = torch.empty(csc.n, dtype=torch.int32, device="cuda") if i % 3 else np.empty(csc.n, dtype=np.uint32)
+        outs.append(o)
+        tickets.append(srv.submit_bfs(gid, s, out=o))
+    ids = set()
+    for _ in range(len(srcs) + 1):
+        got = srv.next_done(60)
+        assert got is not None and got[1].status == 0
+        ids.add(got[0])
+    assert ids == {t.id for t in tickets} | {first.id}
+    assert max(t.info().batch_size for t in tickets) > 1
+    for s, o in zip(srcs, outs):
+        got = o.cpu().numpy().view(np.uint32) if isinstance(o, torch.Tensor) else o
+        np.testing.assert_array_equal(got, O.bfs_csc(csc.n, csc.col_ptrs, csc.rows, s))
+    st = srv.stats()
+    assert st["requests_mbfs"] + st["jobs_bfs"] == len(srcs)
     srv.close()
 
 
