@@ -220,13 +220,38 @@ def profiled_traffic(workload: str):
     return float(entry["bytes_per_launch"]) if entry else None
 
 
-def bfs_config(workload, n, nnz, nsrc, edges_per_step, slices, world):
+L2_LARGE = "inputs larger than L2 (BVSS+CSR in HBM), no flush"
+
+
+def bfs_config(workload, n, nnz, nsrc, edges_per_step, slices, world, l2=L2_LARGE):
     """Workload keys of a BFS line, the same for both arms."""
     return {"workload": workload, "description": WORKLOADS[workload][5], "n": int(n), "nnz_directed": int(nnz),
             "undirected_edges": int(nnz) // 2, "sources_per_step": int(nsrc),
             "reached_edges_per_step": int(edges_per_step), "bvss_slices": int(slices),
-            "l2": "inputs larger than L2 (BVSS+CSR in HBM), no flush",
-            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+            "l2": l2, "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+
+
+class L2Flush:
+    """Between timed steps, for a graph that fits in L2: writes a buffer of
+    twice the L2 size on the timing stream, outside the steps' events, so
+    every step starts with the graph out of L2. A no-op for larger graphs."""
+
+    def __init__(self, graph_bytes: int, stream, dev: int):
+        import torch
+        l2 = int(torch.cuda.get_device_properties(dev).L2_cache_size)
+        self.active = graph_bytes < 2 * l2
+        self.stream = stream
+        self.buf = torch.empty(2 * l2 // 4, dtype=torch.int32, device="cuda") if self.active else None
+        self.note = (f"graph {graph_bytes / 1e6:.1f} MB fits in L2 ({l2 / 1e6:.0f} MB): L2 flushed between timed "
+                     f"steps (a {2 * l2 / 1e6:.0f} MB write outside the timed events)" if self.active else L2_LARGE)
+        self.count = 0
+
+    def __call__(self) -> None:
+        if self.active:
+            import torch
+            self.count += 1
+            with torch.cuda.stream(self.stream):
+                self.buf.fill_(self.count)
 
 
 def cc_config(workload, n, nnz, slices, components, world):
@@ -711,8 +736,6 @@ def run_serving(args, rank, world):
     # result buffers, recycled once a result has been consumed: pinned host
     # memory (the result crosses PCIe) or device memory (it stays in HBM for
     # a consumer on the GPU)
-    import queue as qmod
-
     def make_pools(device: bool):
         """Result buffers per graph: enough that the client rarely waits for
         one (it waits only when every buffer of a graph holds a request in
@@ -726,12 +749,12 @@ def run_serving(args, rank, world):
             cap = min(args.host_pool_gb * 1e9, 0.25 * psutil.virtual_memory().available / len(graphs))
         pools = []
         for _, csc, _, _, _ in graphs:
-            q = qmod.Queue()
+            q = []
             for _ in range(max(8, min(args.buffers, int(cap // (4 * csc.n))))):
                 if device:
-                    q.put(torch.empty(csc.n, dtype=torch.int32, device="cuda"))
+                    q.append(torch.empty(csc.n, dtype=torch.int32, device="cuda"))
                 else:
-                    q.put(torch.empty(csc.n, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32))
+                    q.append(torch.empty(csc.n, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32))
             pools.append(q)
         return pools
 
@@ -787,13 +810,16 @@ def run_serving(args, rank, world):
 def serving_sweep(args, graphs, pools, rates, Server):
     """Open-loop Poisson arrivals at each rate; returns one record per rate.
 
-    Request i is due at its Poisson arrival time; the client submits it then
-    (or, if every result buffer of its graph is in flight, as soon as one is
-    recycled: the wait is counted as client stall and as latency). A
-    consumer thread takes finished tickets from the server's completion
-    queue in completion order and recycles their buffers at once. Latency
-    p50/p99 run from the due time to completion (open loop); the server's
-    own figures (from submission) are reported beside them."""
+    Request i is due at its Poisson arrival time and the client submits it
+    then, into a free result buffer of its graph. When every buffer of that
+    graph holds a request in flight, the request waits in the graph's
+    client-side backlog (arrivals for the other graphs go on) and is
+    submitted as soon as a buffer of its graph is recycled. A consumer
+    thread takes finished tickets from the server's completion queue in
+    completion order and recycles their buffers at once. Latency p50/p99 run
+    from the due time to completion (open loop, backlog wait included); the
+    server's own figures (from submission) are reported beside them."""
+    import collections
     import threading
     rng = np.random.default_rng(SEED)
     sweep = []
@@ -804,10 +830,25 @@ def serving_sweep(args, graphs, pools, rates, Server):
         gaps = rng.exponential(1.0 / lam, nreq)
         kinds = rng.random(nreq) < 0.8
         which = rng.integers(0, len(graphs), nreq)
+        pick = rng.integers(0, 1 << 30, nreq)  # source of a BFS request: pick % pool size
         inflight = {}  # ticket id -> (graph index, pool source index, buffer, client delay s)
+        backlog = [collections.deque() for _ in graphs]  # (request, due) waiting for a buffer
+        free = [list(p) for p in pools]
         lock = threading.Lock()
         lat, edges, failed = [], [0], [0]
         left = [nreq]
+        waited = [0, 0.0]  # requests that waited for a buffer, their summed wait
+
+        def submit(i, buf, due):  # with the lock held
+            gi = int(which[i])
+            si = -1
+            if kinds[i]:
+                src = graphs[gi][4]
+                si = int(pick[i] % len(src))
+                t = srv.submit_bfs(gids[gi], int(src[si]), out=buf)
+            else:
+                t = srv.submit_cc(gids[gi], out=buf)
+            inflight[t.id] = (gi, si, buf, time.perf_counter() - due)
 
         def consume():
             while True:
@@ -819,24 +860,25 @@ def serving_sweep(args, graphs, pools, rates, Server):
                     continue
                 tid, info = got
                 with lock:
-                    while tid not in inflight:  # submit() returned but not yet recorded
-                        lock.release()
-                        time.sleep(0)
-                        lock.acquire()
                     gi, si, buf, delay = inflight.pop(tid)
                     left[0] -= 1
+                    if backlog[gi]:
+                        j, due_j = backlog[gi].popleft()
+                        waited[0] += 1
+                        waited[1] += time.perf_counter() - due_j
+                        submit(j, buf, due_j)
+                    else:
+                        free[gi].append(buf)
+                srv.release(tid)
                 if info.status != 0:
                     failed[0] += 1
                 else:
                     lat.append(info.done_s - info.submit_s + delay)
                     if si >= 0:
                         edges[0] += int(graphs[gi][3][si])
-                pools[gi].put(buf)
-                srv.release(tid)
 
         cons = threading.Thread(target=consume)
         cons.start()
-        stall = 0.0
         t_start = time.perf_counter()
         due = t_start
         for i in range(nreq):
@@ -844,21 +886,16 @@ def serving_sweep(args, graphs, pools, rates, Server):
             while time.perf_counter() < due:
                 pass
             gi = int(which[i])
-            try:
-                buf = pools[gi].get_nowait()
-            except Exception:
-                t0 = time.perf_counter()
-                buf = pools[gi].get()
-                stall += time.perf_counter() - t0
-            si = -1
             with lock:
-                if kinds[i]:
-                    src = graphs[gi][4]
-                    si = int(rng.integers(0, len(src)))
-                    t = srv.submit_bfs(gids[gi], int(src[si]), out=buf)
+                if free[gi]:
+                    submit(i, free[gi].pop(), due)
                 else:
-                    t = srv.submit_cc(gids[gi], out=buf)
-                inflight[t.id] = (gi, si, buf, time.perf_counter() - due)
+                    backlog[gi].append((i, due))
+        while True:  # the backlog drains through the consumer
+            with lock:
+                if left[0] == 0:
+                    break
+            time.sleep(0.001)
         srv.drain(600)
         wall = time.perf_counter() - t_start
         cons.join()
@@ -870,7 +907,8 @@ def serving_sweep(args, graphs, pools, rates, Server):
                       "p50_ms": pct(0.50), "p99_ms": pct(0.99), "mean_ms": round(float(lat_ms.mean()), 3),
                       "server_p50_ms": round(st["p50_latency_s"] * 1e3, 3),
                       "server_p99_ms": round(st["p99_latency_s"] * 1e3, 3),
-                      "client_stall_s": round(stall, 3), "jobs": st["jobs"],
+                      "waited_for_buffer": waited[0], "buffer_wait_s": round(waited[1], 3),
+                      "buffers": [len(p) for p in pools], "jobs": st["jobs"],
                       "batched_requests": st["batched_requests"], "rejected": st["rejected"],
                       "failed": failed[0],
                       "jobs_by_kind": {"bfs": st["jobs_bfs"], "mbfs": st["jobs_mbfs"], "cc": st["jobs_cc"]},
@@ -956,6 +994,7 @@ def run_b200(args, rank, world):
         for _ in range(count):
             ws.sync_one()
 
+    flush = L2Flush(int(info.device_bytes_graph), stream, dev)
     for _ in range(args.warmup):
         step()
         settle(len(sources))
@@ -965,10 +1004,13 @@ def run_b200(args, rank, world):
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     torch.cuda.synchronize()
+    flush()
     with ClockSampler(dev) as clocks:
         t0.record(stream)
         for k in range(args.steps):
             step(per_bfs[k])
+            if k + 1 < args.steps:
+                flush()
             if k:
                 settle(len(sources))  # step k - 1 (step k keeps the GPU busy)
         t1.record(stream)
@@ -976,7 +1018,9 @@ def run_b200(args, rank, world):
     ws.sync()
     barrier()
     torch.cuda.synchronize()
-    ms = t0.elapsed_time(t1)
+    # with flushes, the timed region is the steps alone (first BFS start to
+    # last BFS end of each step)
+    ms = (sum(evs[0][0].elapsed_time(evs[-1][1]) for evs in per_bfs) if flush.active else t0.elapsed_time(t1))
     bfs_ms = [e[0].elapsed_time(e[1]) for evs in per_bfs for e in evs]
     ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if world > 1:
@@ -1074,7 +1118,8 @@ def run_b200(args, rank, world):
         "value": round(value, 3), "unit": "GTEPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generator; see config)",
-        "config": bfs_config(args.workload, n, csc.nnz, len(sources), edges_per_step, info.no_slices, world),
+        "config": bfs_config(args.workload, n, csc.nnz, len(sources), edges_per_step, info.no_slices, world,
+                             flush.note),
         "impl_detail": {"bfs_params": tuned or f"defaults (alpha 14, beta 24, occupancy grid, "
                                                  f"{args.slice_test} slice test, direction {args.direction})",
                         "device_tiles": int(info.device_tiles),
@@ -1356,7 +1401,10 @@ def run_reference(args, rank, world):
         "value": round(value, 3), "unit": "GTEPS", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(tot_t * 1e3 / args.steps, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generator; see config)",
-        "config": bfs_config(args.workload, n, nnz, len(sources), sum(mr.values()), slices, 1),
+        "config": bfs_config(args.workload, n, nnz, len(sources), sum(mr.values()), slices, 1,
+                             L2_LARGE if 5 * slices + 4 * nnz > 252e6 else
+                             "each stock hostCode call uploads the graph first (BFS/BVSSBFSKernel.cuh:1385-1447), "
+                             "which leaves it in L2; no flush"),
         "impl_detail": {"reference_kernel": variant,
                         "timing": "BVSSBFSKernel::hostCode's own time: omp_get_wtime launch -> cudaDeviceSynchronize "
                                   "(BFS/BVSSBFSKernel.cuh:1469,1545-1548)"},

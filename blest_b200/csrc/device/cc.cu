@@ -207,6 +207,10 @@ __global__ void __launch_bounds__(512, 3) cc_persistent_kernel(CcArgs a) {
 #pragma unroll
                         for (int j = 0; j < 8; ++j)
                             if ((hb >> j) & 1u) m = min(m, col[j]);
+                        // labels only fall from the vertex id, so labels[row] <= row:
+                        // m >= row lowers nothing and needs no label read (half the
+                        // slices of the first iteration, where labels are the ids)
+                        if (m >= row) continue;
                         if (m < __ldcg(&a.labels[row])) {
                             // one pointer jump: m is the id of a vertex of the
                             // same component, so its label is a valid, possibly

@@ -86,3 +86,30 @@ def test_algorithmic_bytes_and_reached_edges():
     v_r = int((rp[rsets + 1].astype(np.int64) - rp[rsets]).sum())
     s_r = int((ssp[rp[rsets + 1]].astype(np.int64) - ssp[rp[rsets]].astype(np.int64)).sum())
     assert bench.algorithmic_bytes(a, levels) == 5 * s_r + 12 * v_r + 4 * 4
+
+
+def test_serving_sweep_is_open_loop_with_per_graph_backlogs():
+    """The serving client on a dry-run server: with two result buffers per
+    graph, requests beyond them wait in their graph's backlog (arrivals for
+    the other graph go on) and every request completes exactly once."""
+    from types import SimpleNamespace
+
+    from blest_b200.server import Server
+
+    class DryServer(Server):
+        def __init__(self, **kw):
+            super().__init__(dry_run=True, **kw)
+
+        def add_graph(self, n):
+            return self.add_virtual_graph(n)
+
+    graphs = [("a", None, 1000, np.arange(1, 5, dtype=np.int64), np.arange(4, dtype=np.uint32)),
+              ("b", None, 3000, np.arange(1, 5, dtype=np.int64), np.arange(4, dtype=np.uint32))]
+    pools = [[np.zeros(n, dtype=np.uint32) for _ in range(2)] for _, _, n, _, _ in graphs]
+    args = SimpleNamespace(lanes=1, requests=400, seconds=1.0)
+    rec, = bench.serving_sweep(args, graphs, pools, [4000.0], DryServer)
+    assert rec["requests"] == 400 and rec["failed"] == 0 and rec["rejected"] == 0
+    assert rec["waited_for_buffer"] > 0 and rec["buffers"] == [2, 2]
+    assert rec["jobs"] == sum(rec["jobs_by_kind"].values())
+    assert rec["jobs_by_kind"]["bfs"] + rec["requests_by_kind"]["mbfs"] + rec["requests_by_kind"]["cc"] == 400
+    assert rec["p99_ms"] >= rec["p50_ms"] > 0
