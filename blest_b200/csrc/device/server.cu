@@ -129,8 +129,8 @@ uint64_t job_bytes(const GraphEntry& ge, int kind, const std::vector<Request*>& 
 }
 
 void finish(blest_server* s, Job& job, int status, const std::string& err, double start) {
-    const double t = now(s);
     std::lock_guard<std::mutex> lk(s->mu);
+    const double t = now(s);  // under the lock: done times follow the completion queue's order
     for (Request* r : job.reqs) {
         r->status = status;
         r->error = err;
