@@ -786,28 +786,40 @@ def run_serving(args, rank, world):
     for device_results in modes:
         pools = make_pools(device_results)
         sweeps["device" if device_results else "host"] = serving_sweep(args, graphs, pools, rates, Server)
+        if device_results and args.compare_always and not args.always_batch:
+            # the same device-result sweep with every pending group batched
+            sweeps["device_always"] = serving_sweep(args, graphs, pools, rates, Server, always_batch=True)
         del pools
         torch.cuda.empty_cache()
-    sweep = sweeps.get("host") or sweeps["device"]
+    # value: results in device memory (the result stays in HBM, as `value`
+    # keeps inputs and outputs resident for the other workloads); e2e: every
+    # result copied to pinned host memory
+    sweep = sweeps.get("device") or sweeps["host"]
     head = sweep[min(1, len(sweep) - 1)]
+    host = sweeps.get("host")
+    ehead = host[min(1, len(host) - 1)] if host else None
     return {
-        "metric": "serving p50 latency (ms) at the sweep's second rate; p50/p99 and GTEPS per rate in config.sweep",
+        "metric": "serving p50 latency (ms, open loop: due time to completion) at the sweep's second rate; p50/p99, "
+                  "throughput and GTEPS per rate in config.sweep",
         "value": head["p50_ms"], "unit": "ms", "n_gpus": 1, "steps": len(sweep), "warmup": 0,
         "ms_per_step": None, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic (seeded generators; Poisson arrivals from a fixed seed)",
         "config": {"workload": "serving",
                    "description": (SERVING_FULL_DESCRIPTION if args.serving_full else WORKLOADS["serving"][5]),
                    "graphs": [x[0] for x in graphs], "lanes": args.lanes, "max_batch": 128,
-                   "sweep": sweep, "sweep_device_results": sweeps.get("device"),
-                   "result_memory": "sweep: pinned host buffers (each result crosses PCIe); sweep_device_results: "
-                                    "device buffers (results stay in HBM)"},
-        "e2e": {"value": head["p50_ms"], "unit": "ms", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
-                "note": "latency measured from submit to result in host memory"},
+                   "batch_policy": "always" if args.always_batch else "adaptive",
+                   "sweep": sweep, "sweep_host_results": host,
+                   "sweep_always_batch": sweeps.get("device_always"),
+                   "result_memory": "sweep: device buffers (results stay in HBM for a consumer on the GPU); "
+                                    "sweep_host_results: pinned host buffers (each result crosses PCIe)"},
+        "e2e": ({"value": ehead["p50_ms"], "unit": "ms", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                 "note": "the same sweep with every result copied to pinned host memory; p50 at its second rate"}
+                if ehead else None),
         "parity": parity,
     }
 
 
-def serving_sweep(args, graphs, pools, rates, Server):
+def serving_sweep(args, graphs, pools, rates, Server, always_batch=None):
     """Open-loop Poisson arrivals at each rate; returns one record per rate.
 
     Request i is due at its Poisson arrival time and the client submits it
@@ -824,7 +836,8 @@ def serving_sweep(args, graphs, pools, rates, Server):
     rng = np.random.default_rng(SEED)
     sweep = []
     for lam in rates:
-        srv = Server(lanes=args.lanes, max_batch=128, completion_queue=True)
+        srv = Server(lanes=args.lanes, max_batch=128, completion_queue=True,
+                     always_batch=args.always_batch if always_batch is None else always_batch)
         gids = [srv.add_graph(g) for _, _, g, _, _ in graphs]
         nreq = int(min(args.requests, max(50, lam * args.seconds)))
         gaps = rng.exponential(1.0 / lam, nreq)
@@ -1452,6 +1465,10 @@ def main():
                     help="serving: most result buffers per graph")
     ap.add_argument("--pool-gb", type=float, default=8.0,
                     help="serving: most GB of device result buffers per graph")
+    ap.add_argument("--always-batch", action="store_true",
+                    help="serving: coalesce every group of pending BFS requests (no adaptive policy)")
+    ap.add_argument("--compare-always", action="store_true",
+                    help="serving: also run the device-result sweep with --always-batch, for comparison")
     ap.add_argument("--host-pool-gb", type=float, default=3.0,
                     help="serving: most GB of pinned host result buffers per graph")
     ap.add_argument("--serving-results", choices=["host", "device", "both"], default="both",

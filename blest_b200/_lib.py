@@ -114,7 +114,7 @@ class MbfsStats(C.Structure):
 
 class ServerParams(C.Structure):
     _fields_ = [("memory_budget", u64), ("lanes", u32), ("max_batch", u32), ("queue_capacity", u32),
-                ("dry_run", i32), ("completion_queue", i32)]
+                ("dry_run", i32), ("completion_queue", i32), ("batch_policy", i32)]
 
 
 class QueryResult(C.Structure):
@@ -127,7 +127,8 @@ class ServerStats(C.Structure):
                 ("batched_requests", u64), ("p50_latency_s", f64), ("p99_latency_s", f64),
                 ("mean_latency_s", f64), ("busy_s", f64), ("peak_reserved_bytes", u64), ("memory_budget", u64),
                 ("jobs_bfs", u64), ("jobs_mbfs", u64), ("jobs_cc", u64), ("requests_mbfs", u64),
-                ("requests_cc", u64), ("busy_bfs_s", f64), ("busy_mbfs_s", f64), ("busy_cc_s", f64)]
+                ("requests_cc", u64), ("busy_bfs_s", f64), ("busy_mbfs_s", f64), ("busy_cc_s", f64),
+                ("unbatched_requests", u64)]
 
 
 class MbfsItem(C.Structure):

@@ -5,7 +5,11 @@
 // scheduler thread forms jobs whenever an executor lane is free:
 //  - pending BFS requests on the same graph are coalesced, up to
 //    max_batch, into one multi-source BFS (a lone request uses the
-//    single-source kernel, which has lower latency);
+//    single-source kernel, which has lower latency); under the adaptive
+//    policy a batch runs only when the graph's measured lane time of a
+//    multi-source job of its width is below that of its requests one by
+//    one, else the front request runs alone and the rest stay pending for
+//    the next free lanes;
 //  - pending CC requests on the same graph share one CC run;
 //  - a job is admitted only if its device scratch fits the memory budget
 //    (the batch is shrunk, or the job waits for running jobs to finish;
@@ -60,6 +64,10 @@ struct Request {
 struct GraphEntry {
     blest_graph* g = nullptr;  // null for virtual (dry-run) graphs
     uint32_t n = 0;
+    // running estimates (lane seconds) of a single-source BFS job and of a
+    // multi-source job per width class (32 / 64 / 128 sources), for the
+    // adaptive batch policy; 0 = not measured yet
+    double single_s = 0, mbfs_s[3] = {0, 0, 0};
     uint64_t nnz = 0;
     uint64_t ws_bytes = 0;     // one workspace
 };
@@ -101,7 +109,7 @@ struct blest_server {
     uint32_t lane_grid = 0;
     std::deque<uint64_t> done_q;  // finished tickets (completion_queue servers)
     // stats
-    uint64_t submitted = 0, completed = 0, rejected = 0, jobs = 0, batched = 0;
+    uint64_t submitted = 0, completed = 0, rejected = 0, jobs = 0, batched = 0, unbatched = 0;
     uint64_t kind_jobs[3] = {0, 0, 0}, kind_requests[3] = {0, 0, 0};  // single BFS, multi-source BFS, CC
     double busy_s = 0, kind_busy[3] = {0, 0, 0};
     std::vector<double> latencies;
@@ -116,6 +124,11 @@ double now(const blest_server* s) { return std::chrono::duration<double>(Clock::
 int job_kind(const Job& job) {
     return job.kind == BLEST_QUERY_CC ? 2 : (job.reqs.size() > 1 ? 1 : 0);
 }
+
+// Width class of a multi-source batch of k sources (group width 32/64/128).
+int width_class(size_t k) { return k <= 32 ? 0 : (k <= 64 ? 1 : 2); }
+
+void update_estimate(double& est, double t) { est = est > 0 ? 0.75 * est + 0.25 * t : t; }
 
 // Device bytes a job needs beyond already-resident workspaces: the MBFS
 // state and a staging row per host-bound result (device-bound results are
@@ -143,6 +156,10 @@ void finish(blest_server* s, Job& job, int status, const std::string& err, doubl
         if (s->p.completion_queue) s->done_q.push_back(r->id);
     }
     const int kk = job_kind(job);
+    if (status == BLEST_OK && kk < 2) {
+        GraphEntry& ge = s->graphs[job.graph];
+        update_estimate(kk == 0 ? ge.single_s : ge.mbfs_s[width_class(job.reqs.size())], t - start);
+    }
     ++s->kind_jobs[kk];
     s->kind_requests[kk] += job.reqs.size();
     s->kind_busy[kk] += t - start;
@@ -156,8 +173,10 @@ int run_job(blest_server* s, Lane& lane, Job& job) {
         for (Request* r : job.reqs)
             if (r->out) r->out[0] = (uint32_t)job.reqs.size();  // marks the batch in dry runs
         // stands in for the device time of a job, so that requests arriving
-        // meanwhile queue up behind it as they would behind a real run
-        std::this_thread::sleep_for(std::chrono::microseconds(500));
+        // meanwhile queue up behind it as they would behind a real run: 1 ms
+        // for a single request or a CC run, 5 ms for a multi-source batch
+        const bool batch = job.kind == BLEST_QUERY_BFS && job.reqs.size() > 1;
+        std::this_thread::sleep_for(std::chrono::microseconds(batch ? 5000 : 1000));
         return BLEST_OK;
     }
     cudaSetDevice(s->device);
@@ -251,6 +270,16 @@ bool form_job(blest_server* s, Job& job) {
     if (job.kind == BLEST_QUERY_BFS) {
         while (k > 1 && s->reserved + job_bytes(ge, job.kind, take, k) > s->budget) k = k > 32 ? (k + 1) / 2 : k - 1;
     }
+    // adaptive policy: run the front request alone when the batch would cost
+    // more lane time than its requests one by one (after the shrink, so the
+    // estimate is for the batch that would run)
+    if (job.kind == BLEST_QUERY_BFS && k > 1 && s->p.batch_policy == BLEST_BATCH_ADAPTIVE) {
+        const double m = ge.mbfs_s[width_class(k)];
+        if (ge.single_s > 0 && m > 0 && k * ge.single_s < m) {
+            k = 1;
+            ++s->unbatched;
+        }
+    }
     const uint64_t need = job_bytes(ge, job.kind, take, job.kind == BLEST_QUERY_BFS ? k : 1);
     if (s->reserved + need > s->budget) return false;
     take.resize(job.kind == BLEST_QUERY_BFS ? k : take.size());
@@ -318,6 +347,8 @@ int blest_server_create(const blest_server_params* p, blest_server** out) {
     blest_server* s = nullptr;
     const int rc = guarded([&] {
         blest::require(out, "null argument");
+        blest::require(!p || p->batch_policy == BLEST_BATCH_ADAPTIVE || p->batch_policy == BLEST_BATCH_ALWAYS,
+                       "bad batch_policy");
         s = new blest_server;
         if (p) s->p = *p;
         if (!s->p.lanes) s->p.lanes = 4;
@@ -401,6 +432,13 @@ int blest_server_submit_ex(blest_server* s, uint32_t graph_id, int kind, uint32_
         blest::require(kind == BLEST_QUERY_BFS || kind == BLEST_QUERY_CC, "bad query kind");
         blest::require(out_mem == BLEST_MEM_HOST || out_mem == BLEST_MEM_DEVICE, "bad out_mem");
         blest::require(!(s->p.dry_run && out_mem == BLEST_MEM_DEVICE), "dry-run servers take host buffers only");
+        if (out_mem == BLEST_MEM_DEVICE) {
+            // refused here rather than failing the whole batch it would join
+            cudaPointerAttributes at{};
+            BLEST_CUDA(cudaPointerGetAttributes(&at, out));
+            if (!((at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) && at.device == s->device))
+                throw blest::Error(BLEST_ERR_INVALID_ARG, "out is not device memory of the server's device");
+        }
         std::lock_guard<std::mutex> lk(s->mu);
         blest::require(graph_id < s->graphs.size(), "unknown graph id");
         if (kind == BLEST_QUERY_BFS && source >= s->graphs[graph_id].n)
@@ -519,6 +557,7 @@ int blest_server_stats_get(blest_server* s, blest_server_stats* out) {
         out->busy_bfs_s = s->kind_busy[0];
         out->busy_mbfs_s = s->kind_busy[1];
         out->busy_cc_s = s->kind_busy[2];
+        out->unbatched_requests = s->unbatched;
         std::vector<double> l = s->latencies;
         if (!l.empty()) {
             std::sort(l.begin(), l.end());

@@ -63,8 +63,11 @@ class Ticket:
 
 class Server:
     def __init__(self, lanes: int = 4, max_batch: int = 128, memory_budget: int = 0, queue_capacity: int = 0,
-                 dry_run: bool = False, completion_queue: bool = False):
-        p = L.ServerParams(memory_budget, lanes, max_batch, queue_capacity, int(dry_run), int(completion_queue))
+                 dry_run: bool = False, completion_queue: bool = False, always_batch: bool = False):
+        """always_batch: coalesce every group of pending BFS requests on a
+        graph (BLEST_BATCH_ALWAYS) instead of the adaptive policy."""
+        p = L.ServerParams(memory_budget, lanes, max_batch, queue_capacity, int(dry_run), int(completion_queue),
+                           int(always_batch))
         h = C.c_void_p()
         L.call("blest_server_create", C.byref(p), C.byref(h))
         self._h = h

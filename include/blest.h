@@ -491,7 +491,15 @@ typedef struct blest_server_params {
                                  (exercises the scheduling logic) */
     int completion_queue;     /* != 0: every finished or refused request's ticket is also
                                  queued for blest_server_next_done */
+    int batch_policy;         /* BLEST_BATCH_ADAPTIVE (0) or BLEST_BATCH_ALWAYS */
 } blest_server_params;
+/* Adaptive: pending BFS requests of a graph run as one multi-source BFS
+ * unless the server's running per-graph estimates (lane seconds of a
+ * single-source job, and of a multi-source job of the batch's width) say
+ * that running them one by one costs less; until both are measured, they
+ * are batched. Always: every group of pending requests is batched. */
+#define BLEST_BATCH_ADAPTIVE 0
+#define BLEST_BATCH_ALWAYS 1
 typedef struct blest_query_result {
     int status;               /* BLEST_OK or the error code of the request */
     int kind;                 /* BLEST_QUERY_* */
@@ -514,6 +522,8 @@ typedef struct blest_server_stats {
     uint64_t jobs_bfs, jobs_mbfs, jobs_cc;
     uint64_t requests_mbfs, requests_cc;  /* requests those jobs served */
     double busy_bfs_s, busy_mbfs_s, busy_cc_s;
+    uint64_t unbatched_requests;  /* BFS requests the adaptive policy ran alone
+                                     although others of their graph were pending */
 } blest_server_stats;
 int blest_server_create(const blest_server_params* p, blest_server** out);
 int blest_server_add_graph(blest_server* s, blest_graph* g, uint32_t* graph_id);

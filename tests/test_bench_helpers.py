@@ -106,7 +106,7 @@ def test_serving_sweep_is_open_loop_with_per_graph_backlogs():
     graphs = [("a", None, 1000, np.arange(1, 5, dtype=np.int64), np.arange(4, dtype=np.uint32)),
               ("b", None, 3000, np.arange(1, 5, dtype=np.int64), np.arange(4, dtype=np.uint32))]
     pools = [[np.zeros(n, dtype=np.uint32) for _ in range(2)] for _, _, n, _, _ in graphs]
-    args = SimpleNamespace(lanes=1, requests=400, seconds=1.0)
+    args = SimpleNamespace(lanes=1, requests=400, seconds=1.0, always_batch=False)
     rec, = bench.serving_sweep(args, graphs, pools, [4000.0], DryServer)
     assert rec["requests"] == 400 and rec["failed"] == 0 and rec["rejected"] == 0
     assert rec["waited_for_buffer"] > 0 and rec["buffers"] == [2, 2]

@@ -106,6 +106,42 @@ def test_dry_run_completion_queue_release_and_kind_stats():
         srv2.next_done(0.01)
 
 
+@pytest.mark.parametrize("always", [False, True])
+def test_dry_run_adaptive_policy_runs_small_groups_alone(always):
+    """Dry-run jobs take 1 ms alone and 5 ms batched. Once both are
+    measured, the adaptive policy runs two pending requests one by one
+    (2 ms < 5 ms) but still batches ten (10 ms > 5 ms); BLEST_BATCH_ALWAYS
+    batches both."""
+    srv = Server(lanes=1, max_batch=128, dry_run=True, always_batch=always)
+    g = srv.add_virtual_graph(1000)
+    # a lone request, then ten at once (whatever the scheduler takes first,
+    # the rest queue behind a 1 ms job and run as a batch): both estimates
+    lone = srv.submit_bfs(g, 0)
+    srv.drain(30)
+    boot = [srv.submit_bfs(g, i) for i in range(10)]
+    srv.drain(30)
+    assert lone.info().batch_size == 1 and max(t.info().batch_size for t in boot) > 1
+    small = []
+    for _ in range(4):  # three at a time
+        small += [srv.submit_bfs(g, i) for i in range(3)]
+        srv.drain(30)
+    big = [srv.submit_bfs(g, i) for i in range(11)]
+    srv.drain(30)
+    st = srv.stats()
+    if always:
+        assert st["unbatched_requests"] == 0
+        assert max(t.info().batch_size for t in small) >= 2
+    else:
+        assert st["unbatched_requests"] >= 4
+        assert all(t.info().batch_size == 1 for t in small)
+    assert max(t.info().batch_size for t in big) >= 6
+    with pytest.raises(BlestError):
+        import ctypes as C
+        from blest_b200 import _lib as L
+        bad = L.ServerParams(0, 1, 0, 0, 1, 0, 7)
+        L.call("blest_server_create", C.byref(bad), C.byref(C.c_void_p()))
+
+
 @pytest.mark.gpu
 def test_results_equal_alone_and_in_the_mix(gpu):
     import oracle as O
@@ -212,6 +248,14 @@ def test_batch_with_host_and_device_results(gpu):
         np.testing.assert_array_equal(got, O.bfs_csc(csc.n, csc.col_ptrs, csc.rows, s))
     st = srv.stats()
     assert st["requests_mbfs"] + st["jobs_bfs"] == len(srcs)
+    # a host buffer passed as device memory is refused at submission, before
+    # it could fail the batch it would join
+    import ctypes as C
+    from blest_b200 import _lib as L
+    host = np.empty(csc.n, dtype=np.uint32)
+    with pytest.raises(BlestError):
+        L.call("blest_server_submit_ex", srv._h, gid, L.QUERY_BFS, srcs[0], host.ctypes.data, L.MEM_DEVICE,
+               C.byref(L.u64()))
     srv.close()
 
 
