@@ -521,7 +521,10 @@ int blest_server_next_done(blest_server* s, double timeout_s, uint64_t* ticket, 
         *ticket = s->done_q.front();
         s->done_q.pop_front();
         auto it = s->requests.find(*ticket);
-        if (it != s->requests.end()) fill_result(*it->second, result);
+        if (it != s->requests.end())
+            fill_result(*it->second, result);
+        else if (result)  // released before it was taken from the queue
+            std::memset(result, 0, sizeof(*result));
     });
 }
 

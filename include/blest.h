@@ -543,7 +543,8 @@ int blest_server_drain(blest_server* s, double timeout_s);
 /* Servers created with completion_queue: the ticket of the next request to
  * finish (or be refused), in completion order, with its result record;
  * BLEST_ERR_BUSY when none finishes within timeout_s. Lets a client recycle
- * each result buffer as soon as its request is done, whatever the order. */
+ * each result buffer as soon as its request is done, whatever the order.
+ * (A ticket released before it is taken comes back with a zeroed result.) */
 int blest_server_next_done(blest_server* s, double timeout_s, uint64_t* ticket, blest_query_result* result);
 /* Forget a finished request (its ticket becomes unknown), so a long-running
  * server does not keep a record of every request it has served. */
