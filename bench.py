@@ -1362,7 +1362,7 @@ def run_reference(args, rank, world):
                             ("LazyFullPad" if variant.endswith("FullPad") else "Lazy"),
                             "timing": "BVSSCCKernel::hostCode's own time (launch -> cudaDeviceSynchronize)"},
             "e2e": {"value": round(float(np.mean(walls)) * 1e3, 4), "unit": "ms",
-                    "h2d_bytes_per_step": None, "d2h_bytes_per_step": 4 * n,
+                    "h2d_bytes_per_step": ref.upload_bytes("cc", nnz), "d2h_bytes_per_step": 4 * n,
                     "note": "wall time of the whole stock hostCode call: per-call graph upload, run, label download, "
                             "host relabel"},
             "clocks": clocks.summary(),
@@ -1424,7 +1424,7 @@ def run_reference(args, rank, world):
         "sample": f"{per_step} of the {len(sources)} sources per timed step, rotating ({k} BFS calls); every source "
                   f"ran once before timing",
         "e2e": {"value": round(tot_e / tot_wall / 1e9, 4), "unit": "GTEPS",
-                "h2d_bytes_per_step": None, "d2h_bytes_per_step": 4 * n * per_step,
+                "h2d_bytes_per_step": ref.upload_bytes("bfs", nnz) * per_step, "d2h_bytes_per_step": 4 * n * per_step,
                 "note": "wall time of the whole stock hostCode call: per-call graph upload "
                         "(BFS/BVSSBFSKernel.cuh:1385-1447), run, level download (:1550)"},
         "clocks": clocks.summary(),

@@ -333,15 +333,31 @@ class RefGraph:
                 "slice_set_ptrs": arr(ssp, V.value + 1), "virtual_to_real": arr(v2r, V.value),
                 "real_ptrs": arr(rp, R.value + 1), "row_ids": arr(ri, S.value), "masks": arr(mk, S.value // 4)}
 
-    def bvss_slices(self) -> int:
-        """Slice count of the built BVSS (no array copies)."""
+    def bvss_sizes(self) -> tuple[int, int, int, int]:
+        """(n, real slice sets R, virtual slice sets V, slices S) of the
+        built BVSS (no array copies)."""
         n, R, V = C.c_uint32(), C.c_uint32(), C.c_uint32()
         S = C.c_uint64()
         div = C.c_double()
         ssp, v2r, rp, ri, mk = P64(), P32(), P32(), P32(), P32()
         _rcheck(rlib().ref_bvss_get(self.h, C.byref(n), C.byref(R), C.byref(V), C.byref(S), C.byref(div),
                                     C.byref(ssp), C.byref(v2r), C.byref(rp), C.byref(ri), C.byref(mk)))
-        return S.value
+        return n.value, R.value, V.value, S.value
+
+    def bvss_slices(self) -> int:
+        """Slice count of the built BVSS (no array copies)."""
+        return self.bvss_sizes()[3]
+
+    def upload_bytes(self, kind: str, nnz: int) -> int:
+        """Bytes the reference's stock hostCode copies host -> device on every
+        call: the BVSS arrays (slice-set pointers 8 B, virtual-to-real 4 B
+        per vset, real pointers, 4-byte row ids, one mask word per 4
+        slices), plus for BFS the pull CSR (BFS/BVSSBFSKernel.cuh:1394-1401)
+        and for CC the initial labels and vset queue
+        (CC/BVSSCCKernel.cuh:1154-1203)."""
+        n, R, V, S = self.bvss_sizes()
+        b = 8 * (V + 1) + 4 * V + 4 * (R + 1) + 4 * S + S
+        return b + (4 * (n + 1) + 4 * nnz if kind == "bfs" else 4 * n + 4 * V)
 
     def bfs_variant(self) -> int:
         v = C.c_int()

@@ -125,3 +125,18 @@ def test_oracle_generator_equals_the_library(kind):
     np.testing.assert_array_equal(cp, c.col_ptrs)
     np.testing.assert_array_equal(rw, c.rows)
     np.testing.assert_array_equal(O.sample_sources(n, cp, 40, 11), c.sample_sources(40, 11))
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference harness not built")
+def test_reference_upload_bytes_follow_its_arrays():
+    """The reference arm's e2e byte count: what the stock hostCode copies to
+    the device per call, from the sizes of the reference's own arrays."""
+    n, cp, rw = O.gen_rmat(10, 8, seed=2, permute_seed=3)
+    g = O.RefGraph.from_csc(n, cp, rw)
+    g.reorder("jaccard", 256)
+    g.build_bvss(full_padding=False)
+    a = g.bvss()
+    bvss = sum(a[k].nbytes for k in ("slice_set_ptrs", "virtual_to_real", "real_ptrs", "row_ids", "masks"))
+    nnz = int(cp[-1])
+    assert g.upload_bytes("bfs", nnz) == bvss + 4 * (n + 1) + 4 * nnz
+    assert g.upload_bytes("cc", nnz) == bvss + 4 * n + 4 * a["virtual_to_real"].size
