@@ -237,6 +237,10 @@ std::vector<uint32_t> ordering_load_bin(const std::string& path, uint32_t n) {
     return inv;
 }
 
+// Parallel without atomics or sorting: thread t owns the rows of range t
+// and scans every column in increasing order, counting (then writing) only
+// the entries of its rows, so each transposed list is filled in increasing
+// column order, as the sequential loop does.
 Csc csc_transpose(const Csc& g) {
     Csc t;
     t.n = g.n;
@@ -244,25 +248,50 @@ Csc csc_transpose(const Csc& g) {
     t.is_social = g.is_social;
     t.col_ptrs.assign((size_t)g.n + 1, 0);
     t.rows.resize(g.nnz);
-    for (uint32_t p = 0; p < g.nnz; ++p) ++t.col_ptrs[g.rows[p] + 1];
-    for (uint32_t i = 1; i <= g.n; ++i) t.col_ptrs[i] += t.col_ptrs[i - 1];
-    std::vector<uint32_t> cursor(t.col_ptrs.begin(), t.col_ptrs.end() - 1);
-    // Columns visited in increasing j, so every transposed list is sorted.
-    for (uint32_t j = 0; j < g.n; ++j)
-        for (uint32_t p = g.col_ptrs[j]; p < g.col_ptrs[j + 1]; ++p) t.rows[cursor[g.rows[p]]++] = j;
+    const uint32_t n = g.n;
+    const uint32_t* rows = g.rows.data();
+    const uint32_t* cp = g.col_ptrs.data();
+    uint32_t* tp = t.col_ptrs.data();
+    uint32_t* tr = t.rows.data();
+#pragma omp parallel
+    {
+        const uint32_t T = (uint32_t)omp_get_num_threads(), me = (uint32_t)omp_get_thread_num();
+        const uint32_t lo = (uint32_t)((uint64_t)n * me / T), hi = (uint32_t)((uint64_t)n * (me + 1) / T);
+        const uint32_t span = hi - lo;
+        for (uint32_t p = 0; p < g.nnz; ++p)
+            if (rows[p] - lo < span) ++tp[rows[p] + 1];
+#pragma omp barrier
+#pragma omp single
+        for (uint32_t i = 1; i <= n; ++i) tp[i] += tp[i - 1];
+        std::vector<uint32_t> cursor(tp + lo, tp + hi);
+        for (uint32_t j = 0; j < n; ++j)
+            for (uint32_t p = cp[j]; p < cp[j + 1]; ++p) {
+                const uint32_t r = rows[p] - lo;
+                if (r < span) tr[cursor[r]++] = j;
+            }
+    }
     return t;
 }
 
+// Every off-diagonal (i, j) has its (j, i): columns checked in parallel
+// (binary search in the sorted column i), stopping early on the first miss.
 bool csc_check_symmetry(const Csc& g) {
-    for (uint32_t j = 0; j < g.n; ++j) {
+    int ok = 1;
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (int64_t jj = 0; jj < (int64_t)g.n; ++jj) {
+        if (!__atomic_load_n(&ok, __ATOMIC_RELAXED)) continue;
+        const uint32_t j = (uint32_t)jj;
         for (uint32_t p = g.col_ptrs[j]; p < g.col_ptrs[j + 1]; ++p) {
             const uint32_t i = g.rows[p];
             if (i == j) continue;
             const auto b = g.rows.begin() + g.col_ptrs[i], e = g.rows.begin() + g.col_ptrs[i + 1];
-            if (!std::binary_search(b, e, j)) return false;
+            if (!std::binary_search(b, e, j)) {
+                __atomic_store_n(&ok, 0, __ATOMIC_RELAXED);
+                break;
+            }
         }
     }
-    return true;
+    return ok != 0;
 }
 
 Csc csc_symmetrize(const Csc& g) {

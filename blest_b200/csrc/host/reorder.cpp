@@ -7,6 +7,8 @@
 
 #include <omp.h>
 
+#include <parallel/algorithm>
+
 #include <algorithm>
 #include <numeric>
 
@@ -191,15 +193,23 @@ namespace {
 // a vertex's discoverer is the first vertex in queue order that has it as
 // a neighbour, at its first adjacency position; a parent's children are
 // appended in adjacency order (then, if `sort_children`, reordered by the
-// same std::sort on ascending degree as the reference). Levels with many
-// vertices are processed in parallel: every parent claims its unmarked
-// neighbours with an atomic minimum of (queue position, adjacency index),
-// the claims are counted per parent, prefix-summed into positions and
-// written; small levels run the sequential loop itself.
+// same std::sort on ascending degree as the reference). Small levels run
+// the sequential loop itself. A large level runs in parallel one of two
+// ways, whichever scans fewer edges:
+//  - top-down: every parent claims its unmarked neighbours with an atomic
+//    minimum of (queue position, adjacency index); the claims are counted
+//    per parent, prefix-summed into positions and written (three passes
+//    over the level's edges);
+//  - bottom-up (once the unreached vertices' edges, plus a check of every
+//    vertex, cost less than those three passes): every unreached vertex takes the smallest queue position among
+//    its neighbours (on a symmetric graph every reached neighbour of an
+//    unreached vertex lies in the current level, so that is its
+//    discoverer), and the new level is sorted by (that position, vertex
+//    id) — the same order, because adjacency lists are sorted by id.
 class OrderedBfs {
 public:
     OrderedBfs(const uint32_t* ptrs, const uint32_t* inds, const uint32_t* degrees, uint32_t n)
-        : ptrs_(ptrs), inds_(inds), deg_(degrees), key_(n, ~0ull) {}
+        : ptrs_(ptrs), inds_(inds), deg_(degrees), n_(n), key_(n, ~0ull), pos_(n, kNone) {}
 
     // BFS from q[qs] (already marked); `unmarked(v)` / `mark(v)` give the
     // visited state. Fills q from qs on; returns the end and the start of
@@ -210,11 +220,16 @@ public:
         uint32_t ls = qs, le = qs + 1;
         levels = 1;
         last_level = ls;
+        // edges of the vertices not reached yet (for the direction choice),
+        // counted at the first large level only: a run over a small
+        // component (RMAT graphs have many) costs nothing in n
+        uint64_t rest = 0;
+        bool counted = false;
         auto degAsc = [this](uint32_t a, uint32_t b) { return deg_[a] < deg_[b]; };
+        uint64_t work = deg_[q[qs]];  // edges of the level being expanded
         for (;;) {
-            uint64_t work = 0;
-            for (uint32_t i = ls; i < le && work < kParallelWork; ++i) work += ptrs_[q[i] + 1] - ptrs_[q[i]];
             uint32_t ne = le;
+            uint64_t next = 0;  // edges of the new level (each pass adds them up)
             if (work < kParallelWork) {
                 for (uint32_t i = ls; i < le; ++i) {
                     const uint32_t u = q[i];
@@ -224,59 +239,28 @@ public:
                         if (unmarked(v)) {
                             mark(v);
                             q[ne++] = v;
+                            next += deg_[v];
                         }
                     }
                     if (sort_children) std::sort(q.begin() + first, q.begin() + ne, degAsc);
                 }
             } else {
-                const int64_t L = (int64_t)le - ls;
-                cnt_.assign((size_t)L + 1, 0);
-#pragma omp parallel for schedule(dynamic, 64)
-                for (int64_t x = 0; x < L; ++x) {
-                    const uint32_t u = q[ls + x];
-                    for (uint32_t p = ptrs_[u]; p < ptrs_[u + 1]; ++p) {
-                        const uint32_t v = inds_[p];
-                        if (!unmarked(v)) continue;
-                        const uint64_t k = ((uint64_t)(ls + x) << 32) | (p - ptrs_[u]);
-                        uint64_t cur = __atomic_load_n(&key_[v], __ATOMIC_RELAXED);
-                        while (k < cur &&
-                               !__atomic_compare_exchange_n(&key_[v], &cur, k, true, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
-                        }
-                    }
+                if (!counted) {
+#pragma omp parallel for reduction(+ : rest) schedule(static, 65536)
+                    for (int64_t v = 0; v < (int64_t)n_; ++v)
+                        if (unmarked((uint32_t)v)) rest += deg_[v];
+                    counted = true;
                 }
-#pragma omp parallel for schedule(dynamic, 64)
-                for (int64_t x = 0; x < L; ++x) {
-                    const uint32_t u = q[ls + x];
-                    uint32_t c = 0;
-                    for (uint32_t p = ptrs_[u]; p < ptrs_[u + 1]; ++p) {
-                        const uint32_t v = inds_[p];
-                        if (unmarked(v) && key_[v] == (((uint64_t)(ls + x) << 32) | (p - ptrs_[u]))) ++c;
-                    }
-                    cnt_[x + 1] = c;
-                }
-                for (int64_t x = 0; x < L; ++x) cnt_[x + 1] += cnt_[x];
-                ne = le + (uint32_t)cnt_[L];
-#pragma omp parallel for schedule(dynamic, 64)
-                for (int64_t x = 0; x < L; ++x) {
-                    const uint32_t u = q[ls + x];
-                    uint32_t w = le + (uint32_t)cnt_[x];
-                    const uint32_t first = w;
-                    for (uint32_t p = ptrs_[u]; p < ptrs_[u + 1]; ++p) {
-                        const uint32_t v = inds_[p];
-                        if (unmarked(v) && key_[v] == (((uint64_t)(ls + x) << 32) | (p - ptrs_[u]))) q[w++] = v;
-                    }
-                    if (sort_children) std::sort(q.begin() + first, q.begin() + w, degAsc);
-                }
-#pragma omp parallel for schedule(static, 4096)
-                for (int64_t i = le; i < (int64_t)ne; ++i) {
-                    const uint32_t v = q[i];
-                    key_[v] = ~0ull;
-                    mark(v);
-                }
+                // bottom-up reads every unreached vertex's edges plus a flag
+                // per vertex; top-down makes three passes over the level's edges
+                if (rest + n_ / 4 < 3 * work) ne = bottom_up(q, ls, le, sort_children, unmarked, mark, degAsc, next);
+                else ne = top_down(q, ls, le, sort_children, unmarked, mark, degAsc, next);
             }
+            if (counted) rest -= std::min(rest, next);
             if (ne == le) break;
             ls = le;
             le = ne;
+            work = next;
             last_level = ls;
             ++levels;
         }
@@ -284,12 +268,125 @@ public:
     }
 
 private:
+    template <class Unmarked, class Mark, class Cmp>
+    uint32_t top_down(std::vector<uint32_t>& q, uint32_t ls, uint32_t le, bool sort_children, Unmarked unmarked,
+                      Mark mark, Cmp degAsc, uint64_t& next) {
+        const int64_t L = (int64_t)le - ls;
+        cnt_.assign((size_t)L + 1, 0);
+#pragma omp parallel for schedule(dynamic, 64)
+        for (int64_t x = 0; x < L; ++x) {
+            const uint32_t u = q[ls + x];
+            for (uint32_t p = ptrs_[u]; p < ptrs_[u + 1]; ++p) {
+                const uint32_t v = inds_[p];
+                if (!unmarked(v)) continue;
+                const uint64_t k = ((uint64_t)(ls + x) << 32) | (p - ptrs_[u]);
+                uint64_t cur = __atomic_load_n(&key_[v], __ATOMIC_RELAXED);
+                while (k < cur &&
+                       !__atomic_compare_exchange_n(&key_[v], &cur, k, true, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
+                }
+            }
+        }
+#pragma omp parallel for schedule(dynamic, 64)
+        for (int64_t x = 0; x < L; ++x) {
+            const uint32_t u = q[ls + x];
+            uint32_t c = 0;
+            for (uint32_t p = ptrs_[u]; p < ptrs_[u + 1]; ++p) {
+                const uint32_t v = inds_[p];
+                if (unmarked(v) && key_[v] == (((uint64_t)(ls + x) << 32) | (p - ptrs_[u]))) ++c;
+            }
+            cnt_[x + 1] = c;
+        }
+        for (int64_t x = 0; x < L; ++x) cnt_[x + 1] += cnt_[x];
+        const uint32_t ne = le + (uint32_t)cnt_[L];
+#pragma omp parallel for schedule(dynamic, 64)
+        for (int64_t x = 0; x < L; ++x) {
+            const uint32_t u = q[ls + x];
+            uint32_t w = le + (uint32_t)cnt_[x];
+            const uint32_t first = w;
+            for (uint32_t p = ptrs_[u]; p < ptrs_[u + 1]; ++p) {
+                const uint32_t v = inds_[p];
+                if (unmarked(v) && key_[v] == (((uint64_t)(ls + x) << 32) | (p - ptrs_[u]))) q[w++] = v;
+            }
+            if (sort_children) std::sort(q.begin() + first, q.begin() + w, degAsc);
+        }
+        uint64_t sum = 0;
+#pragma omp parallel for reduction(+ : sum) schedule(static, 4096)
+        for (int64_t i = le; i < (int64_t)ne; ++i) {
+            const uint32_t v = q[i];
+            key_[v] = ~0ull;
+            mark(v);
+            sum += deg_[v];
+        }
+        next = sum;
+        return ne;
+    }
+
+    template <class Unmarked, class Mark, class Cmp>
+    uint32_t bottom_up(std::vector<uint32_t>& q, uint32_t ls, uint32_t le, bool sort_children, Unmarked unmarked,
+                       Mark mark, Cmp degAsc, uint64_t& next) {
+        // queue positions of the current level: every reached neighbour of
+        // an unreached vertex is in it (cleared again below)
+#pragma omp parallel for schedule(static, 4096)
+        for (int64_t i = ls; i < (int64_t)le; ++i) pos_[q[i]] = (uint32_t)i;
+        const int T = omp_get_max_threads();
+        if ((int)part_.size() < T) part_.resize(T);
+        std::vector<size_t> off((size_t)T + 1, 0);
+#pragma omp parallel num_threads(T)
+        {
+            std::vector<uint64_t>& mine = part_[omp_get_thread_num()];
+            mine.clear();
+            // static: thread t takes a contiguous range, so the parts are in id order
+#pragma omp for schedule(static)
+            for (int64_t v = 0; v < (int64_t)n_; ++v) {
+                if (!unmarked((uint32_t)v)) continue;
+                uint32_t best = kNone;
+                for (uint32_t p = ptrs_[v]; p < ptrs_[v + 1]; ++p) best = std::min(best, pos_[inds_[p]]);
+                if (best != kNone) mine.push_back(((uint64_t)best << 32) | (uint64_t)v);
+            }
+        }
+        for (int t = 0; t < T; ++t) off[t + 1] = off[t] + part_[t].size();
+        level_.resize(off[T]);
+#pragma omp parallel for schedule(static, 1) num_threads(T)
+        for (int t = 0; t < T; ++t) std::copy(part_[t].begin(), part_[t].end(), level_.begin() + off[t]);
+        __gnu_parallel::sort(level_.begin(), level_.end());
+#pragma omp parallel for schedule(static, 4096)
+        for (int64_t i = ls; i < (int64_t)le; ++i) pos_[q[i]] = kNone;
+        const int64_t K = (int64_t)level_.size();
+        const uint32_t ne = le + (uint32_t)K;
+        uint64_t sum = 0;
+#pragma omp parallel for reduction(+ : sum) schedule(static, 4096)
+        for (int64_t i = 0; i < K; ++i) {
+            const uint32_t v = (uint32_t)level_[i];
+            q[le + i] = v;
+            mark(v);
+            sum += deg_[v];
+        }
+        next = sum;
+        if (sort_children) {
+            // each parent's children (one run of equal positions, in id =
+            // adjacency order) get the reference's degree sort
+#pragma omp parallel for schedule(dynamic, 1024)
+            for (int64_t i = 0; i < K; ++i) {
+                if (i > 0 && (level_[i] >> 32) == (level_[i - 1] >> 32)) continue;
+                int64_t j = i + 1;
+                while (j < K && (level_[j] >> 32) == (level_[i] >> 32)) ++j;
+                if (j - i > 1) std::sort(q.begin() + le + i, q.begin() + le + j, degAsc);
+            }
+        }
+        return ne;
+    }
+
     static constexpr uint64_t kParallelWork = 1u << 16;  // edges of a level worth a parallel pass
+    static constexpr uint32_t kNone = 0xFFFFFFFFu;
     const uint32_t* ptrs_;
     const uint32_t* inds_;
     const uint32_t* deg_;
+    uint32_t n_;
     std::vector<uint64_t> key_;
+    std::vector<uint32_t> pos_;  // queue positions of the level a bottom-up step expands, else kNone
     std::vector<uint64_t> cnt_;
+    std::vector<std::vector<uint64_t>> part_;
+    std::vector<uint64_t> level_;
 };
 
 }  // namespace

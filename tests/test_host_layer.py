@@ -167,10 +167,16 @@ def test_relabel_dense():
 @pytest.mark.skipif(not O.ref_available(), reason="reference harness not built")
 @pytest.mark.parametrize("make", [lambda: Csc.rmat(16, 16, seed=2, permute_seed=2),
                                   lambda: Csc.er(1 << 16, 16 << 15, seed=3),
-                                  lambda: Csc.grid(300, 200, 0.3, 0.001, seed=3)])
+                                  lambda: Csc.grid(300, 200, 0.3, 0.001, seed=3),
+                                  lambda: Csc.er(1 << 18, 16 << 18, seed=4),
+                                  lambda: Csc.rmat(17, 16, seed=6, permute_seed=3)],
+                         ids=["rmat16", "er16", "grid300x200", "er18_deg32", "rmat17"])
 def test_rcm_matches_reference_on_parallel_levels(make):
-    """RCM orders big enough that levels run on the parallel path (more
-    than 2^16 edges per level) equal the reference's sequential order."""
+    """RCM orders big enough that levels run on the parallel paths (more
+    than 2^16 edges per level: top-down claims, and bottom-up steps once the
+    unreached vertices hold fewer edges than the level) equal the
+    reference's sequential order, including the many small components of
+    RMAT graphs."""
     c = make()
     want = O.RefGraph.from_csc(c.n, c.col_ptrs, c.rows).reorder("rcm")
     np.testing.assert_array_equal(c.reorder("rcm"), want)
@@ -191,3 +197,36 @@ def test_gorder_matches_reference(make):
     want = O.RefGraph.from_csc(c.n, c.col_ptrs, c.rows).reorder("gorder")
     got = c.reorder("gorder")
     np.testing.assert_array_equal(np.asarray(got), want)
+
+
+def test_transpose_and_symmetry_check_on_directed_input():
+    """The parallel transpose gives every transposed list in increasing
+    column order (duplicates kept), as a sequential fill would; the parallel
+    symmetry check finds a single missing reverse edge."""
+    rng = np.random.default_rng(7)
+    n = 3000
+    src = rng.integers(0, n, 40000)
+    dst = rng.integers(0, n, 40000)
+    order = np.lexsort((dst, src))
+    src, dst = src[order], dst[order]
+    ptrs = np.concatenate([[0], np.cumsum(np.bincount(src, minlength=n))]).astype(np.uint32)
+    g = Csc.from_arrays(n, ptrs, dst.astype(np.uint32))
+    t = g.transpose()
+    cols = np.repeat(np.arange(n), np.diff(g.col_ptrs.astype(np.int64)))
+    want = np.lexsort((cols, g.rows))
+    np.testing.assert_array_equal(t.rows, cols[want])
+    np.testing.assert_array_equal(t.col_ptrs, np.concatenate([[0], np.cumsum(np.bincount(g.rows, minlength=n))]))
+    assert not g.is_symmetric()
+    s = Csc.rmat(12, 8, seed=1, permute_seed=1)
+    assert s.is_symmetric()
+    # drop one reverse edge of the last column: asymmetric again
+    cp, rw = s.col_ptrs.astype(np.int64), s.rows.copy()
+    j = s.n - 1
+    while cp[j + 1] == cp[j]:
+        j -= 1
+    keep = np.ones(rw.size, dtype=bool)
+    keep[cp[j + 1] - 1] = False
+    ptrs2 = cp.copy()
+    ptrs2[j + 1:] -= 1
+    a = Csc.from_arrays(s.n, ptrs2.astype(np.uint32), rw[keep])
+    assert not a.is_symmetric()
