@@ -349,36 +349,82 @@ void csc_apply_permutation(Csc& g, const std::vector<uint32_t>& inv) {
     g.rows.swap(rows);
 }
 
+// Symmetrised, de-duplicated, self-loop-free CSC of an edge stream, built
+// without random-access atomics: the edges are drawn twice per thread (each
+// thread a fixed range of edge indices) — once to count both directions per
+// vertex partition (a few thousand consecutive-id partitions), once to write
+// them as packed (vertex, neighbour) pairs into their partition's slice of
+// one buffer — and each partition then fills, sorts and de-duplicates its
+// own columns with counters that stay in cache. Columns are sorted and
+// unique, so the arrays do not depend on the thread count or write order.
 Csc csc_from_undirected_edges(uint32_t n, uint64_t m, const EdgeFn& edge) {
-    std::vector<uint32_t> deg((size_t)n + 1, 0);
-#pragma omp parallel for schedule(static, 1 << 16)
-    for (int64_t e = 0; e < (int64_t)m; ++e) {
-        uint32_t u, v;
-        if (!edge((uint64_t)e, &u, &v) || u == v) continue;
-        __atomic_fetch_add(&deg[u], 1u, __ATOMIC_RELAXED);
-        __atomic_fetch_add(&deg[v], 1u, __ATOMIC_RELAXED);
+    uint32_t shift = 0;  // partition of vertex u: u >> shift, at most 4096 partitions
+    while (((uint64_t)n >> shift) > 4096) ++shift;
+    const uint32_t P = (uint32_t)((((uint64_t)n - 1) >> shift) + 1);
+    const int T = omp_get_max_threads();
+    std::vector<uint64_t> cnt((size_t)T * P, 0);  // [thread][partition]
+#pragma omp parallel num_threads(T)
+    {
+        const int t = omp_get_thread_num(), nt = omp_get_num_threads();
+        const uint64_t e0 = m * t / nt, e1 = m * (t + 1) / nt;
+        uint64_t* c = cnt.data() + (size_t)t * P;
+        for (uint64_t e = e0; e < e1; ++e) {
+            uint32_t u, v;
+            if (!edge(e, &u, &v) || u == v) continue;
+            ++c[u >> shift];
+            ++c[v >> shift];
+        }
     }
-    std::vector<uint64_t> raw((size_t)n + 1, 0);
-    for (uint32_t j = 0; j < n; ++j) raw[j + 1] = raw[j] + deg[j];
-    const uint64_t total = raw[n];
-    std::vector<uint32_t> tmp(total);
-    std::vector<uint64_t> cursor(raw.begin(), raw.end() - 1);
-#pragma omp parallel for schedule(static, 1 << 16)
-    for (int64_t e = 0; e < (int64_t)m; ++e) {
-        uint32_t u, v;
-        if (!edge((uint64_t)e, &u, &v) || u == v) continue;
-        tmp[__atomic_fetch_add(&cursor[u], 1ull, __ATOMIC_RELAXED)] = v;
-        tmp[__atomic_fetch_add(&cursor[v], 1ull, __ATOMIC_RELAXED)] = u;
+    // partition-major offsets: partition p's pairs, thread by thread
+    std::vector<uint64_t> off((size_t)T * P, 0), pbase((size_t)P + 1, 0);
+    uint64_t total = 0;
+    for (uint32_t p = 0; p < P; ++p) {
+        pbase[p] = total;
+        for (int t = 0; t < T; ++t) {
+            off[(size_t)t * P + p] = total;
+            total += cnt[(size_t)t * P + p];
+        }
     }
-    cursor.clear();
-    cursor.shrink_to_fit();
-    // Sort + unique each column; the column's unique count goes to deg.
-#pragma omp parallel for schedule(dynamic, 1024)
-    for (int64_t j = 0; j < (int64_t)n; ++j) {
-        uint32_t* b = tmp.data() + raw[j];
-        uint32_t* e = tmp.data() + raw[j + 1];
-        std::sort(b, e);
-        deg[j] = (uint32_t)(std::unique(b, e) - b);
+    pbase[P] = total;
+    std::vector<uint64_t> pairs(total);
+#pragma omp parallel num_threads(T)
+    {
+        const int t = omp_get_thread_num(), nt = omp_get_num_threads();
+        const uint64_t e0 = m * t / nt, e1 = m * (t + 1) / nt;
+        uint64_t* o = off.data() + (size_t)t * P;
+        for (uint64_t e = e0; e < e1; ++e) {
+            uint32_t u, v;
+            if (!edge(e, &u, &v) || u == v) continue;
+            pairs[o[u >> shift]++] = ((uint64_t)u << 32) | v;
+            pairs[o[v >> shift]++] = ((uint64_t)v << 32) | u;
+        }
+    }
+    // per partition: neighbours of each of its columns, sorted and unique,
+    // left in place at the front of the column's range of `pairs`
+    std::vector<uint32_t> deg((size_t)n, 0);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t pp = 0; pp < (int64_t)P; ++pp) {
+        const uint32_t p = (uint32_t)pp;
+        const uint32_t lo = p << shift, hi = (uint32_t)std::min<uint64_t>(n, ((uint64_t)p + 1) << shift);
+        const uint32_t w = hi - lo;
+        const uint64_t b = pbase[p], e = pbase[p + 1];
+        std::vector<uint64_t> start((size_t)w + 1, 0);  // column j - lo occupies [start[j-lo], start[j-lo+1])
+        for (uint64_t i = b; i < e; ++i) ++start[(uint32_t)(pairs[i] >> 32) - lo + 1];
+        for (uint32_t j = 0; j < w; ++j) start[j + 1] += start[j];
+        std::vector<uint64_t> cur(start.begin(), start.end() - 1);
+        std::vector<uint32_t> col(e - b);
+        for (uint64_t i = b; i < e; ++i) col[cur[(uint32_t)(pairs[i] >> 32) - lo]++] = (uint32_t)pairs[i];
+        // sorted, unique neighbours written back over the partition's pairs as u32
+        uint32_t* dst = reinterpret_cast<uint32_t*>(pairs.data() + b);
+        for (uint32_t j = 0; j < w; ++j) {
+            uint32_t* cb = col.data() + start[j];
+            uint32_t* ce = col.data() + start[j + 1];
+            std::sort(cb, ce);
+            const uint32_t k = (uint32_t)(std::unique(cb, ce) - cb);
+            deg[lo + j] = k;
+            std::memcpy(dst, cb, 4ull * k);
+            dst += k;
+        }
     }
     uint64_t nnz = 0;
     for (uint32_t j = 0; j < n; ++j) nnz += deg[j];
@@ -389,9 +435,13 @@ Csc csc_from_undirected_edges(uint32_t n, uint64_t m, const EdgeFn& edge) {
     g.col_ptrs.assign((size_t)n + 1, 0);
     for (uint32_t j = 0; j < n; ++j) g.col_ptrs[j + 1] = g.col_ptrs[j] + deg[j];
     g.rows.resize(nnz);
-#pragma omp parallel for schedule(dynamic, 1024)
-    for (int64_t j = 0; j < (int64_t)n; ++j)
-        std::memcpy(g.rows.data() + g.col_ptrs[j], tmp.data() + raw[j], 4ull * deg[j]);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t pp = 0; pp < (int64_t)P; ++pp) {
+        const uint32_t p = (uint32_t)pp;
+        const uint32_t lo = p << shift, hi = (uint32_t)std::min<uint64_t>(n, ((uint64_t)p + 1) << shift);
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(pairs.data() + pbase[p]);
+        std::memcpy(g.rows.data() + g.col_ptrs[lo], src, 4ull * (g.col_ptrs[hi] - g.col_ptrs[lo]));
+    }
     g.is_social = classify_social(g);
     return g;
 }
