@@ -2,6 +2,8 @@
 
 #include <omp.h>
 
+#include <parallel/algorithm>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -60,7 +62,7 @@ bool is_social_degree_distribution(const std::vector<uint32_t>& deg) {
     if (maxDeg == 0 || sumDeg == 0) return false;
 
     std::vector<uint32_t> sorted = deg;
-    std::sort(sorted.begin(), sorted.end());
+    __gnu_parallel::sort(sorted.begin(), sorted.end());
     auto shareTop = [&](double frac) {
         double raw = frac * (double)n;
         uint32_t k = (uint32_t)std::ceil(raw);
@@ -116,8 +118,14 @@ bool is_social_degree_distribution(const std::vector<uint32_t>& deg) {
 bool classify_social(const Csc& g) {
     std::vector<uint32_t> outDeg(g.n), inDeg(g.n, 0);
     for (uint32_t j = 0; j < g.n; ++j) outDeg[j] = g.degree(j);
-    for (uint32_t p = 0; p < g.nnz; ++p)
-        if (g.rows[p] < g.n) ++inDeg[g.rows[p]];
+    // in-degrees without atomics: each thread counts the rows of its range
+#pragma omp parallel
+    {
+        const uint32_t T = (uint32_t)omp_get_num_threads(), me = (uint32_t)omp_get_thread_num();
+        const uint32_t lo = (uint32_t)((uint64_t)g.n * me / T), hi = (uint32_t)((uint64_t)g.n * (me + 1) / T);
+        for (uint32_t p = 0; p < g.nnz; ++p)
+            if (g.rows[p] - lo < hi - lo) ++inDeg[g.rows[p]];
+    }
     bool social = is_social_degree_distribution(inDeg) || is_social_degree_distribution(outDeg);
     return social || (g.average_degree() > kSocialThreshold);
 }
