@@ -136,38 +136,190 @@ static void sort_columns(Csc& g) {
         std::sort(g.rows.begin() + g.col_ptrs[j], g.rows.begin() + g.col_ptrs[j + 1]);
 }
 
-Csc csc_read_mtx(const std::string& path, bool undirected, bool binary) {
-    std::ifstream file(path);
-    if (!file.is_open()) throw Error(BLEST_ERR_IO, "cannot open Matrix Market file: " + path);
-    while (file.peek() == '%') file.ignore(1 << 20, '\n');
-    uint32_t n = 0, n2 = 0;
-    uint64_t lines = 0;
-    if (!(file >> n >> n2 >> lines)) throw Error(BLEST_ERR_IO, "bad Matrix Market size line: " + path);
-    std::vector<std::vector<uint32_t>> adj(n);
-    uint64_t nnz = 0;
-    for (uint64_t it = 0; it < lines; ++it) {
-        uint64_t j, i;
-        double trash;
-        if (!(file >> j >> i)) throw Error(BLEST_ERR_IO, "truncated Matrix Market file: " + path);
-        if (!binary && !(file >> trash)) throw Error(BLEST_ERR_IO, "missing value in Matrix Market entry: " + path);
-        if (i == j) continue;
-        if (i == 0 || j == 0 || i > n || j > n) throw Error(BLEST_ERR_IO, "Matrix Market index out of range: " + path);
-        adj[j - 1].push_back((uint32_t)(i - 1));
-        ++nnz;
-        if (undirected) {
-            adj[i - 1].push_back((uint32_t)(j - 1));
-            ++nnz;
+namespace {
+
+inline bool mtx_space(char c) { return c == ' ' || c == '\t' || c == '\n' || c == '\r' || c == '\v' || c == '\f'; }
+
+// Unsigned decimal token at buf[p] (after whitespace); false if it is not one.
+inline bool mtx_uint(const char* buf, size_t size, size_t& p, uint64_t& out) {
+    while (p < size && mtx_space(buf[p])) ++p;
+    if (p < size && buf[p] == '+') ++p;
+    if (p >= size || buf[p] < '0' || buf[p] > '9') return false;
+    uint64_t v = 0;
+    while (p < size && buf[p] >= '0' && buf[p] <= '9') {
+        v = v * 10 + (uint64_t)(buf[p] - '0');
+        ++p;
+    }
+    out = v;
+    return p >= size || mtx_space(buf[p]);
+}
+
+// A numeric value token at buf[p] (after whitespace); false if there is none.
+inline bool mtx_value(const char* buf, size_t size, size_t& p) {
+    while (p < size && mtx_space(buf[p])) ++p;
+    if (p >= size) return false;
+    char* e = nullptr;
+    std::strtod(buf + p, &e);
+    if (e == buf + p || (e < buf + size && !mtx_space(*e))) return false;
+    p = (size_t)(e - buf);
+    return true;
+}
+
+// CSC with sorted columns (duplicates kept) from per-thread lists of packed
+// (column << 32 | row) pairs: pairs are bucketed by column partition, then
+// every partition counts, fills and sorts its own columns.
+Csc csc_from_column_pairs(uint32_t n, std::vector<std::vector<uint64_t>>& parts) {
+    uint32_t shift = 0;
+    while (((uint64_t)n >> shift) > 4096) ++shift;
+    const uint32_t P = n ? (uint32_t)((((uint64_t)n - 1) >> shift) + 1) : 1;
+    const int T = (int)parts.size();
+    std::vector<uint64_t> off((size_t)T * P, 0), pbase((size_t)P + 1, 0);
+#pragma omp parallel for schedule(static, 1)
+    for (int t = 0; t < T; ++t)
+        for (uint64_t x : parts[t]) ++off[(size_t)t * P + (uint32_t)(x >> (32 + shift))];
+    uint64_t total = 0;
+    for (uint32_t q = 0; q < P; ++q) {
+        pbase[q] = total;
+        for (int t = 0; t < T; ++t) {
+            const uint64_t c = off[(size_t)t * P + q];
+            off[(size_t)t * P + q] = total;
+            total += c;
         }
     }
-    if (nnz > 0xFFFFFFFFull) throw Error(BLEST_ERR_UNSUPPORTED, "more than 2^32-1 non-zeros");
+    pbase[P] = total;
+    if (total > 0xFFFFFFFFull) throw Error(BLEST_ERR_UNSUPPORTED, "more than 2^32-1 non-zeros");
+    std::vector<uint64_t> pairs(total);
+#pragma omp parallel for schedule(static, 1)
+    for (int t = 0; t < T; ++t) {
+        uint64_t* o = off.data() + (size_t)t * P;
+        for (uint64_t x : parts[t]) pairs[o[(uint32_t)(x >> (32 + shift))]++] = x;
+        std::vector<uint64_t>().swap(parts[t]);
+    }
     Csc g;
     g.n = n;
-    g.nnz = (uint32_t)nnz;
+    g.nnz = (uint32_t)total;
     g.col_ptrs.assign((size_t)n + 1, 0);
-    for (uint32_t j = 0; j < n; ++j) g.col_ptrs[j + 1] = g.col_ptrs[j] + (uint32_t)adj[j].size();
-    g.rows.resize(nnz);
-    for (uint32_t j = 0; j < n; ++j) std::copy(adj[j].begin(), adj[j].end(), g.rows.begin() + g.col_ptrs[j]);
-    sort_columns(g);
+    g.rows.resize(total);
+    // column counts, each partition over its own pairs
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t qq = 0; qq < (int64_t)P; ++qq)
+        for (uint64_t i = pbase[qq]; i < pbase[qq + 1]; ++i) ++g.col_ptrs[(uint32_t)(pairs[i] >> 32) + 1];
+    for (uint32_t j = 0; j < n; ++j) g.col_ptrs[j + 1] += g.col_ptrs[j];
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t qq = 0; qq < (int64_t)P; ++qq) {
+        const uint32_t q = (uint32_t)qq;
+        const uint32_t lo = q << shift, hi = (uint32_t)std::min<uint64_t>(n, ((uint64_t)q + 1) << shift);
+        if (lo >= hi) continue;
+        std::vector<uint32_t> cur(g.col_ptrs.begin() + lo, g.col_ptrs.begin() + hi);
+        for (uint64_t i = pbase[q]; i < pbase[q + 1]; ++i) {
+            const uint64_t x = pairs[i];
+            g.rows[cur[(uint32_t)(x >> 32) - lo]++] = (uint32_t)x;
+        }
+        for (uint32_t j = lo; j < hi; ++j) std::sort(g.rows.begin() + g.col_ptrs[j], g.rows.begin() + g.col_ptrs[j + 1]);
+    }
+    return g;
+}
+
+}  // namespace
+
+// The reference's reader (CSC.cuh:98-185) as a parallel parser with the same
+// token semantics as its stream loop: leading '%' lines skipped, then
+// whitespace-separated tokens "n n' entries" and per entry "j i" (+ a value
+// unless the matrix is a pattern); an entry j i adds row i-1 to column j-1
+// (and column i-1 gets row j-1 when undirected); self loops are dropped
+// before the range check; duplicates are kept; columns end sorted. The file
+// is read whole and cut into per-thread chunks at token boundaries; a
+// thread takes the entries whose first token lies in its chunk (reading on
+// past its end to finish the last one), so token k of the body is entry
+// k / tokens-per-entry whatever the chunking.
+Csc csc_read_mtx(const std::string& path, bool undirected, bool binary) {
+    std::ifstream file(path, std::ios::binary);
+    if (!file.is_open()) throw Error(BLEST_ERR_IO, "cannot open Matrix Market file: " + path);
+    file.seekg(0, std::ios::end);
+    const size_t size = (size_t)file.tellg();
+    file.seekg(0);
+    std::vector<char> data(size + 1, '\0');
+    if (size && !file.read(data.data(), (std::streamsize)size)) throw Error(BLEST_ERR_IO, "short read from " + path);
+    const char* buf = data.data();
+    size_t pos = 0;
+    while (pos < size && buf[pos] == '%') {
+        while (pos < size && buf[pos] != '\n') ++pos;
+        if (pos < size) ++pos;
+    }
+    uint64_t n64 = 0, n2 = 0, lines = 0;
+    if (!mtx_uint(buf, size, pos, n64) || !mtx_uint(buf, size, pos, n2) || !mtx_uint(buf, size, pos, lines) ||
+        n64 > 0xFFFFFFFFull)
+        throw Error(BLEST_ERR_IO, "bad Matrix Market size line: " + path);
+    const uint32_t n = (uint32_t)n64;
+    const uint32_t K = binary ? 2 : 3;  // tokens per entry
+    const int T = std::max(1, omp_get_max_threads());
+    // chunk t = [cut[t], cut[t+1]), each cut moved forward to a token boundary
+    std::vector<size_t> cut((size_t)T + 1);
+    for (int t = 0; t <= T; ++t) {
+        size_t c = pos + (size - pos) * (size_t)t / (size_t)T;
+        while (t > 0 && c < size && c > pos && !mtx_space(buf[c - 1])) ++c;
+        cut[t] = std::min(c, size);
+    }
+    cut[T] = size;
+    std::vector<uint64_t> tok((size_t)T + 1, 0);  // token starts per chunk, then prefix
+#pragma omp parallel for schedule(static, 1) num_threads(T)
+    for (int t = 0; t < T; ++t) {
+        uint64_t c = 0;
+        for (size_t p = cut[t]; p < cut[t + 1]; ++p)
+            c += !mtx_space(buf[p]) && (p == pos || mtx_space(buf[p - 1]));
+        tok[t + 1] = c;
+    }
+    for (int t = 0; t < T; ++t) tok[t + 1] += tok[t];
+    // first failing entry (sequential reading order) and its message
+    std::vector<uint64_t> badAt((size_t)T, ~0ull);
+    std::vector<int> badKind((size_t)T, 0);  // 1 truncated, 2 missing value, 3 index out of range
+    std::vector<std::vector<uint64_t>> parts((size_t)T);
+#pragma omp parallel for schedule(static, 1) num_threads(T)
+    for (int t = 0; t < T; ++t) {
+        std::vector<uint64_t>& out = parts[t];
+        uint64_t k = tok[t];
+        size_t p = cut[t];
+        while (k < (uint64_t)lines * K) {
+            // next token start in this chunk
+            while (p < cut[t + 1] && mtx_space(buf[p])) ++p;
+            if (p >= cut[t + 1]) break;
+            if (k % K != 0) {  // a token of an entry begun in the previous chunk
+                while (p < size && !mtx_space(buf[p])) ++p;
+                ++k;
+                continue;
+            }
+            const uint64_t entry = k / K;
+            uint64_t j = 0, i = 0;
+            size_t q = p;
+            int bad = 0;
+            if (!mtx_uint(buf, size, q, j) || !mtx_uint(buf, size, q, i)) bad = 1;
+            else if (!binary && !mtx_value(buf, size, q)) bad = 2;
+            else if (i != j && (i == 0 || j == 0 || i > n || j > n)) bad = 3;
+            if (bad) {
+                badAt[t] = entry;
+                badKind[t] = bad;
+                break;
+            }
+            if (i != j) {
+                out.push_back(((j - 1) << 32) | (i - 1));
+                if (undirected) out.push_back(((i - 1) << 32) | (j - 1));
+            }
+            // step past this entry's first token only; its other tokens are
+            // skipped above as non-first tokens (they may lie in the next chunk)
+            while (p < size && !mtx_space(buf[p])) ++p;
+            ++k;
+        }
+    }
+    int t0 = -1;
+    for (int t = 0; t < T; ++t)
+        if (badAt[t] != ~0ull && (t0 < 0 || badAt[t] < badAt[t0])) t0 = t;
+    if (t0 < 0 && tok[T] < (uint64_t)lines * K) throw Error(BLEST_ERR_IO, "truncated Matrix Market file: " + path);
+    if (t0 >= 0) {
+        if (badKind[t0] == 2) throw Error(BLEST_ERR_IO, "missing value in Matrix Market entry: " + path);
+        if (badKind[t0] == 3) throw Error(BLEST_ERR_IO, "Matrix Market index out of range: " + path);
+        throw Error(BLEST_ERR_IO, "truncated Matrix Market file: " + path);
+    }
+    Csc g = csc_from_column_pairs(n, parts);
     g.is_social = classify_social(g);
     return g;
 }

@@ -230,3 +230,78 @@ def test_transpose_and_symmetry_check_on_directed_input():
     ptrs2[j + 1:] -= 1
     a = Csc.from_arrays(s.n, ptrs2.astype(np.uint32), rw[keep])
     assert not a.is_symmetric()
+
+
+def _mtx_expected(text: str, undirected: bool, binary: bool):
+    """The reader's semantics restated: leading '%' lines skipped, then a
+    whitespace token stream 'n n entries' and per entry 'j i [value]'; self
+    loops dropped before the range check, duplicates kept, columns sorted."""
+    lines = text.split("\n")
+    k = 0
+    while k < len(lines) and lines[k].startswith("%"):
+        k += 1
+    tok = "\n".join(lines[k:]).split()
+    n, entries = int(tok[0]), int(tok[2])
+    per = 2 if binary else 3
+    cols = [[] for _ in range(n)]
+    body = tok[3:]
+    if len(body) < entries * per:
+        return None
+    for e in range(entries):
+        j, i = int(body[e * per]), int(body[e * per + 1])
+        if i == j:
+            continue
+        cols[j - 1].append(i - 1)
+        if undirected:
+            cols[i - 1].append(j - 1)
+    ptr = np.concatenate([[0], np.cumsum([len(c) for c in cols])]).astype(np.uint32)
+    rows = np.array([r for c in cols for r in sorted(c)], dtype=np.uint32)
+    return ptr, rows
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_mtx_reader_token_stream_any_layout(tmp_path, seed):
+    """The parallel reader cuts the file into per-thread chunks at token
+    boundaries: entries split across lines or chunks, several entries on a
+    line, tabs, CRLF, blank lines, self loops with out-of-range ids and
+    trailing tokens all read as the sequential token stream does."""
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(3, 40))
+    m = int(rng.integers(1, 300))
+    binary = bool(seed % 2)
+    undirected = seed % 3 == 0
+    toks = []
+    for _ in range(m):
+        j, i = int(rng.integers(1, n + 1)), int(rng.integers(1, n + 1))
+        if rng.random() < 0.05:
+            j = i = n + 7  # self loop out of range: dropped before the range check
+        toks += [str(j), str(i)] + ([] if binary else [f"{rng.normal():.3e}"])
+    seps = [" ", "\t", "\n", "\r\n", "  \n\n", " \t "]
+    body = "".join(t + seps[int(rng.integers(0, len(seps)))] for t in toks)
+    text = "%%MatrixMarket matrix coordinate x general\n% comment\n" + f"{n} {n} {m}\n" + body + "99 98\n"
+    p = tmp_path / "g.mtx"
+    p.write_bytes(text.encode())
+    want = _mtx_expected(text, undirected, binary)
+    c = Csc.read_mtx(str(p), undirected=undirected, binary=binary)
+    np.testing.assert_array_equal(c.col_ptrs, want[0])
+    np.testing.assert_array_equal(c.rows, want[1])
+
+
+def test_mtx_reader_errors_follow_the_first_bad_entry(tmp_path):
+    p = tmp_path / "e.mtx"
+    head = "%%MatrixMarket matrix coordinate real general\n"
+    # a value that is not a number
+    p.write_text(head + "3 3 3\n1 2 0.5\n2 3 x\n3 1 1.0\n")
+    with pytest.raises(BlestError, match="missing value"):
+        Csc.read_mtx(str(p), undirected=False, binary=False)
+    # out of range before a later truncation
+    p.write_text(head + "3 3 3\n1 9 0.5\n2 3 1.0\n")
+    with pytest.raises(BlestError, match="out of range"):
+        Csc.read_mtx(str(p), undirected=False, binary=False)
+    # truncated
+    p.write_text(head + "3 3 3\n1 2 0.5\n2 3 1.0\n3\n")
+    with pytest.raises(BlestError, match="truncated"):
+        Csc.read_mtx(str(p), undirected=False, binary=False)
+    p.write_text(head + "3 x 3\n")
+    with pytest.raises(BlestError, match="size line"):
+        Csc.read_mtx(str(p), undirected=False, binary=False)
