@@ -815,6 +815,7 @@ def run_serving(args, rank, world):
         "e2e": ({"value": ehead["p50_ms"], "unit": "ms", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
                  "note": "the same sweep with every result copied to pinned host memory; p50 at its second rate"}
                 if ehead else None),
+        "clocks": head.get("clocks"),
         "parity": parity,
     }
 
@@ -892,25 +893,26 @@ def serving_sweep(args, graphs, pools, rates, Server, always_batch=None):
 
         cons = threading.Thread(target=consume)
         cons.start()
-        t_start = time.perf_counter()
-        due = t_start
-        for i in range(nreq):
-            due += gaps[i]
-            while time.perf_counter() < due:
-                pass
-            gi = int(which[i])
-            with lock:
-                if free[gi]:
-                    submit(i, free[gi].pop(), due)
-                else:
-                    backlog[gi].append((i, due))
-        while True:  # the backlog drains through the consumer
-            with lock:
-                if left[0] == 0:
-                    break
-            time.sleep(0.001)
-        srv.drain(600)
-        wall = time.perf_counter() - t_start
+        with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+            t_start = time.perf_counter()
+            due = t_start
+            for i in range(nreq):
+                due += gaps[i]
+                while time.perf_counter() < due:
+                    pass
+                gi = int(which[i])
+                with lock:
+                    if free[gi]:
+                        submit(i, free[gi].pop(), due)
+                    else:
+                        backlog[gi].append((i, due))
+            while True:  # the backlog drains through the consumer
+                with lock:
+                    if left[0] == 0:
+                        break
+                time.sleep(0.001)
+            srv.drain(600)
+            wall = time.perf_counter() - t_start
         cons.join()
         st = srv.stats()
         lat_ms = np.sort(np.array(lat)) * 1e3
@@ -929,7 +931,7 @@ def serving_sweep(args, graphs, pools, rates, Server, always_batch=None):
                                            "cc": st["requests_cc"]},
                       "lane_busy_s": {"bfs": round(st["busy_bfs_s"], 3), "mbfs": round(st["busy_mbfs_s"], 3),
                                       "cc": round(st["busy_cc_s"], 3)},
-                      "bfs_gteps": round(edges[0] / wall / 1e9, 3)})
+                      "bfs_gteps": round(edges[0] / wall / 1e9, 3), "clocks": clocks.summary()})
         log(f"[serving] rate {lam}/s: {sweep[-1]}")
         srv.close()
     return sweep
