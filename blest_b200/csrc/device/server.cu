@@ -174,9 +174,9 @@ int run_job(blest_server* s, Lane& lane, Job& job) {
             if (r->out) r->out[0] = (uint32_t)job.reqs.size();  // marks the batch in dry runs
         // stands in for the device time of a job, so that requests arriving
         // meanwhile queue up behind it as they would behind a real run: 1 ms
-        // for a single request or a CC run, 5 ms for a multi-source batch
+        // for a single request or a CC run, 20 ms for a multi-source batch
         const bool batch = job.kind == BLEST_QUERY_BFS && job.reqs.size() > 1;
-        std::this_thread::sleep_for(std::chrono::microseconds(batch ? 5000 : 1000));
+        std::this_thread::sleep_for(std::chrono::microseconds(batch ? 20000 : 1000));
         return BLEST_OK;
     }
     cudaSetDevice(s->device);
