@@ -168,7 +168,15 @@ void finish(blest_server* s, Job& job, int status, const std::string& err, doubl
 }
 
 int run_job(blest_server* s, Lane& lane, Job& job) {
-    const GraphEntry& ge = s->graphs[job.graph];
+    // copies taken under the lock: blest_server_add_graph may grow the graph
+    // and workspace tables while this job runs
+    GraphEntry ge;
+    blest_workspace* ws = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        ge = s->graphs[job.graph];
+        ws = lane.ws[job.graph];
+    }
     if (s->p.dry_run) {
         for (Request* r : job.reqs)
             if (r->out) r->out[0] = (uint32_t)job.reqs.size();  // marks the batch in dry runs
@@ -180,14 +188,13 @@ int run_job(blest_server* s, Lane& lane, Job& job) {
         return BLEST_OK;
     }
     cudaSetDevice(s->device);
-    if (!lane.ws[job.graph]) {
-        blest_workspace* ws = nullptr;
+    if (!ws) {
         const int rc = blest_workspace_create(ge.g, &ws);
         if (rc != BLEST_OK) return rc;
         blest_workspace_set_grid(ws, s->lane_grid);
+        std::lock_guard<std::mutex> lk(s->mu);
         lane.ws[job.graph] = ws;
     }
-    blest_workspace* ws = lane.ws[job.graph];
     if (job.kind == BLEST_QUERY_CC) {
         const Request& r0 = *job.reqs[0];
         int rc = blest_cc_ws(ws, r0.out, r0.out_mem, lane.stream, nullptr);
