@@ -272,3 +272,33 @@ def test_request_that_never_fits_is_refused(gpu):
     # batches cannot be admitted; single-source queries need no extra scratch
     assert all(t.info().status == 0 and t.info().batch_size == 1 for t in ts)
     srv.close()
+
+
+def test_dry_run_graphs_added_while_jobs_run():
+    """Adding graphs (which grows the server's graph and workspace tables)
+    while other jobs run leaves every request served."""
+    srv = Server(lanes=3, max_batch=16, dry_run=True)
+    g0 = srv.add_virtual_graph(500)
+    tickets = []
+    stop = threading.Event()
+
+    def client():
+        i = 0
+        while not stop.is_set():
+            tickets.append(srv.submit_bfs(g0, i % 500))
+            i += 1
+            time.sleep(0.0002)
+
+    th = threading.Thread(target=client)
+    th.start()
+    added = []
+    for k in range(40):
+        gid = srv.add_virtual_graph(100 + k)
+        added.append(gid)
+        tickets.append(srv.submit_cc(gid))
+        tickets.append(srv.submit_bfs(gid, k % (100 + k)))
+    stop.set()
+    th.join()
+    srv.drain(60)
+    assert all(t.info().status == 0 for t in tickets)
+    assert srv.stats()["completed"] == len(tickets)
