@@ -134,7 +134,8 @@ class Server:
                                   r.batch_size, r.submit_s, r.start_s, r.done_s)
 
     def release(self, ticket: int) -> None:
-        """Forget a finished request's record."""
+        """Forget a finished request's record (its Ticket can no longer be
+        polled or waited on; the result buffer stays the caller's)."""
         L.call("blest_server_release", self._h, ticket)
 
     def drain(self, timeout_s: float = 600.0) -> None:
