@@ -487,8 +487,9 @@ typedef struct blest_server_params {
     uint32_t lanes;           /* concurrent executors; 0 = 4 */
     uint32_t max_batch;       /* sources per multi-source batch, <= 128; 0 = 128 */
     uint32_t queue_capacity;  /* pending requests; 0 = 2^20 (BLEST_ERR_BUSY beyond) */
-    int dry_run;              /* != 0: no GPU; jobs finish at once and out[0] = batch size
-                                 (exercises the scheduling logic) */
+    int dry_run;              /* != 0: no GPU; each job takes a fixed stand-in time (1 ms,
+                                 20 ms for a multi-source batch) and sets out[0] = batch
+                                 size (exercises the scheduling logic) */
     int completion_queue;     /* != 0: every finished or refused request's ticket is also
                                  queued for blest_server_next_done */
     int batch_policy;         /* BLEST_BATCH_ADAPTIVE (0) or BLEST_BATCH_ALWAYS */
